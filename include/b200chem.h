@@ -1,0 +1,200 @@
+/*
+ * b200chem.h -- C ABI of the B200 (sm_100a) constant-pressure stiff-chemistry
+ * reactor.  It replaces, for one GPU, the per-cell HP reaction advance that
+ * PeleLMeX drives through pele::physics::reactions::ReactorBase:
+ *
+ *   ReactorBase::create(name)        Source/PeleLMeX_Setup.cpp:152-153
+ *   ReactorBase::init(type, ncells)  Source/PeleLMeX_Setup.cpp:146-154
+ *   ReactorBase::set_typ_vals_ode(v) Source/PeleLMeX_Utils.cpp:1472
+ *   ReactorBase::react(box, ...)     Source/PeleLMeX_Reactions.cpp:101-108,267-274
+ *   ReactorBase::close()             Source/PeleLMeX.cpp:26
+ *
+ * Plain C types only: pointers, sizes, and a cudaStream_t passed as void*.
+ * All state arrays are DEVICE pointers in CGS units (the caller converts from
+ * MKS exactly as Source/PeleLMeX_Reactions.cpp:69-79 does).  Every entry point
+ * returns 0 on success and a negative B200CHEM_E* code on failure; the text of
+ * the last error of the calling thread is available from b200chem_last_error().
+ */
+#ifndef B200CHEM_H
+#define B200CHEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200CHEM_VERSION 1
+
+/* ---------------------------------------------------------------- errors */
+#define B200CHEM_OK 0
+#define B200CHEM_EINVAL (-1)     /* bad argument                              */
+#define B200CHEM_ECUDA (-2)      /* a CUDA runtime call failed                */
+#define B200CHEM_ENOMEM (-3)     /* device allocation failed                  */
+#define B200CHEM_EINTEGRATE (-4) /* at least one cell failed to integrate     */
+#define B200CHEM_ETOOBIG (-5)    /* size above a compiled-in limit            */
+
+/* ------------------------------------------------------- per-cell status */
+#define B200CHEM_CELL_OK 0
+#define B200CHEM_CELL_MASKED 1        /* mask == 0: left untouched, fctCount=0  */
+#define B200CHEM_CELL_MAXSTEPS (-1)   /* cvode.max_substeps exceeded            */
+#define B200CHEM_CELL_ERRFAIL (-2)    /* repeated error-test failures / h_min   */
+#define B200CHEM_CELL_CONVFAIL (-3)   /* repeated Newton failures / h_min       */
+#define B200CHEM_CELL_NONFINITE (-4)  /* NaN/Inf or non-positive rho or T input */
+#define B200CHEM_CELL_SINGULAR (-5)   /* iteration matrix singular repeatedly   */
+
+/* ------------------------------------------------------------ mechanism
+ * Flat description of a gas-phase kinetics mechanism in the Chemkin formalism
+ * (CGS-mol-K).  Produced from a mechanism file by pelelmex_b200.mechanism.
+ * This is the data that a CEPTR-generated mechanism.cpp bakes into code
+ * (productionRate, aJacobian, ckhms/ckcpms; reached from PeleLMeX through
+ * eos.RTY2WDOT / eos.T2Hi / eos.HY2T, Source/PeleLMeX_K.H:611,721,880-885). */
+#define B200CHEM_MAX_SLOTS 4 /* distinct species on one side of a reaction */
+
+#define B200CHEM_RXN_ELEMENTARY 0
+#define B200CHEM_RXN_THREEBODY 1
+#define B200CHEM_RXN_LINDEMANN 2
+#define B200CHEM_RXN_TROE 3
+
+#define B200CHEM_RXN_REVERSIBLE 1   /* reverse rate from equilibrium constant */
+#define B200CHEM_RXN_EXPLICIT_REV 2 /* reverse rate from arr_rev              */
+#define B200CHEM_RXN_TROE_T2 4      /* Troe form carries the T** term         */
+
+typedef struct b200chem_mech_desc {
+  int32_t n_species;
+  int32_t n_reactions;
+  int32_t n_eff;          /* number of non-default third-body efficiencies */
+  const double* mw;       /* [N] molecular weight, g/mol */
+  const double* nasa;     /* [N][15] Tmid, low-range a1..a7, high-range a1..a7 */
+  const int32_t* rtype;   /* [R] B200CHEM_RXN_* kind */
+  const int32_t* rflags;  /* [R] B200CHEM_RXN_* flag bits */
+  const double* arr;      /* [R][3] ln A, b, Ea/R (high-pressure limit for falloff) */
+  const double* arr_lo;   /* [R][3] low-pressure limit (falloff kinds only) */
+  const double* arr_rev;  /* [R][3] explicit reverse Arrhenius (flag EXPLICIT_REV) */
+  const double* troe;     /* [R][4] alpha, T***, T*, T** */
+  const int32_t* sp;      /* [R][8] reactant slots 0..3, product slots 4..7; -1 = empty */
+  const int32_t* nu;      /* [R][8] stoichiometric coefficient of each slot (>0) */
+  const int32_t* eff_ptr; /* [R+1] CSR offsets into eff_sp / eff_val */
+  const int32_t* eff_sp;  /* [n_eff] species index of a non-default efficiency */
+  const double* eff_val;  /* [n_eff] its efficiency (all other species: 1) */
+} b200chem_mech_desc;
+
+/* --------------------------------------------------------------- options
+ * ode.rtol, ode.atol, cvode.max_order, cvode.max_substeps keep the meaning
+ * given in Docs/sphinx/manual/LMeXControls.rst:301-310. */
+typedef struct b200chem_opts {
+  double rtol;           /* relative tolerance                                  */
+  double atol;           /* absolute tolerance, or prefactor on typical values  */
+  int32_t max_order;     /* BDF maximum order, 1..5                             */
+  int32_t max_steps;     /* maximum internal steps per cell and call            */
+  int32_t reactor_type;  /* 2 = HP (constant pressure, enthalpy forcing); only 2 */
+  int32_t lu_fp64;       /* 0: FP32 LU + one FP64 refinement step (default); 1: FP64 LU */
+  int32_t warps_per_cta; /* 0: use the autotuned / default launch shape         */
+  int32_t verbose;
+} b200chem_opts;
+
+/* ---------------------------------------------------------- Array4 views
+ * Mirrors amrex::Array4<Real>: element (i,j,k,n) lives at
+ *   p[(i-lo[0]) + (j-lo[1])*jstride + (k-lo[2])*kstride + n*nstride].     */
+typedef struct b200chem_array4 {
+  double* p;
+  int64_t jstride, kstride, nstride;
+  int32_t lo[3], hi[3];
+} b200chem_array4;
+
+typedef struct b200chem_iarray4 {
+  const int32_t* p;
+  int64_t jstride, kstride, nstride;
+  int32_t lo[3], hi[3];
+} b200chem_iarray4;
+
+/* One call of react(box, rhoY, extF_rhoY, T, rhoH, extF_rhoH, fctCount, mask,
+ * ...) from Source/PeleLMeX_Reactions.cpp:101-108.  lo/hi (inclusive) is the
+ * box to advance; the Array4 boxes may be larger (ghost cells). */
+typedef struct b200chem_box_view {
+  int32_t lo[3], hi[3];
+  b200chem_array4 rhoY;      /* N comps, in/out, g/cm^3                 */
+  b200chem_array4 extF_rhoY; /* N comps, in, g/cm^3/s                   */
+  b200chem_array4 T;         /* 1 comp,  in/out, K                       */
+  b200chem_array4 rhoH;      /* 1 comp,  in/out, erg/cm^3                */
+  b200chem_array4 extF_rhoH; /* 1 comp,  in, erg/cm^3/s                  */
+  b200chem_array4 fctCount;  /* 1 comp,  out, RHS evaluations per cell   */
+  b200chem_iarray4 mask;     /* 1 comp,  in, 0 = skip; p may be NULL     */
+} b200chem_box_view;
+
+/* Aggregate counters of one react call (sums over integrated cells). */
+typedef struct b200chem_stats {
+  int64_t n_cells, n_masked, n_failed;
+  int64_t nst, nfe, nje, nlu, netf, ncfn;
+  int32_t max_nfe, max_nst;
+} b200chem_stats;
+
+typedef struct b200chem_reactor* b200chem_handle;
+
+/* -------------------------------------------------------------- lifecycle */
+
+/* ReactorBase::create + init (Source/PeleLMeX_Setup.cpp:146-154).  Copies the
+ * mechanism to the current device.  Returns NULL on failure. */
+b200chem_handle b200chem_create(const b200chem_mech_desc* mech, const b200chem_opts* opts);
+
+/* ReactorBase::set_typ_vals_ode (Source/PeleLMeX_Utils.cpp:1472).  n must be
+ * N+1 (species in CGS, then T).  Afterwards atol_k = opts.atol * typ_k;
+ * before the first call atol_k = opts.atol for every component. */
+int b200chem_set_typvals(b200chem_handle h, const double* typ, int32_t n);
+
+/* ReactorBase::react (call site Source/PeleLMeX_Reactions.cpp:101-108).
+ * Advances every unmasked cell of every box by *dt_react, in place, on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).  *time is advanced
+ * by *dt_react.  cell_status (device, optional) receives one int32 per cell in
+ * box order (box 0 cells with i fastest, then box 1, ...).  stats (host,
+ * optional) makes the call synchronous and fills the counters.  Returns
+ * B200CHEM_EINTEGRATE when stats is given and a cell failed. */
+int b200chem_react(b200chem_handle h, const b200chem_box_view* boxes, int32_t nbox,
+                   double* dt_react, double* time, void* stream, int32_t* cell_status,
+                   b200chem_stats* stats);
+
+/* The flat-array form of react (ReactorBase::react(rY, rYsrc, rX, rX_src, dt,
+ * time, ncells, stream) in PelePhysics): component-major arrays of ncells
+ * cells, i.e. rhoY[n*ncells + c].  fctCount may be NULL. */
+int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T,
+                        double* rhoH, const double* extF_rhoH, double* fctCount,
+                        const int32_t* mask, int64_t ncells, double* dt_react, double* time,
+                        void* stream, int32_t* cell_status, b200chem_stats* stats);
+
+/* ReactorBase::close (Source/PeleLMeX.cpp:26). */
+int b200chem_destroy(b200chem_handle h);
+
+const char* b200chem_last_error(void);
+int b200chem_version(void);
+
+/* ------------------------------------------------- mechanism evaluation
+ * Device-side evaluations of the mechanism interface used inside react, for
+ * parity tests and for callers that need them alone.  Cell-major layouts:
+ * y[c*(N+1) + k] holds rhoY_k (k<N) then T; forcing likewise (extF_rhoY then
+ * extF_rhoH). */
+
+/* HP right-hand side: d(rhoY_k)/dt = W_k wdot_k + F_k and the temperature
+ * equation dT/dt = (F_H - sum_k h_k d(rhoY_k)/dt) / (rho cp). */
+int b200chem_eval_rhs(b200chem_handle h, const double* y, const double* forcing, int64_t ncells,
+                      double* ydot, void* stream);
+
+/* Analytic Jacobian d(ydot)/dy of the same system, jac[c*(N+1)^2 + i*(N+1) + j]. */
+int b200chem_eval_jac(b200chem_handle h, const double* y, const double* forcing, int64_t ncells,
+                      double* jac, void* stream);
+
+/* reactionRateRhoY (Source/PeleLMeX_K.H:850-889) in MKS like the caller:
+ * rho from sum rhoY, T from (h, Y) by Newton starting at T, then the mass
+ * production rates.  Component-major arrays of ncells cells; T is updated to
+ * the value consistent with rhoH. */
+int b200chem_inst_rr(b200chem_handle h, const double* rhoY_mks, const double* rhoH_mks,
+                     double* T, double* rhoYdot_mks, int64_t ncells, void* stream);
+
+/* getTfromHY (Source/PeleLMeX_K.H:700-723) in MKS: T from rho, rhoY, rhoH. */
+int b200chem_t_from_hy(b200chem_handle h, const double* rhoY_mks, const double* rhoH_mks,
+                       double* T, int64_t ncells, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200CHEM_H */
