@@ -1,0 +1,93 @@
+"""Loader and ctypes declarations for the in-tree CUDA library libb200chem.so.
+
+The library is the product: there is no CPU or library fallback.  If it is
+missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libb200chem.so"
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_f64p = ctypes.c_void_p  # device pointers are passed as integers
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_order", ctypes.c_int32),
+                ("max_steps", ctypes.c_int32), ("reactor_type", ctypes.c_int32), ("lu_fp64", ctypes.c_int32),
+                ("warps_per_cta", ctypes.c_int32), ("verbose", ctypes.c_int32)]
+
+
+class Array4(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_void_p), ("jstride", ctypes.c_int64), ("kstride", ctypes.c_int64),
+                ("nstride", ctypes.c_int64), ("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3)]
+
+
+class BoxView(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3), ("rhoY", Array4), ("extF_rhoY", Array4),
+                ("T", Array4), ("rhoH", Array4), ("extF_rhoH", Array4), ("fctCount", Array4), ("mask", Array4)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("n_cells", ctypes.c_int64), ("n_masked", ctypes.c_int64), ("n_failed", ctypes.c_int64),
+                ("nst", ctypes.c_int64), ("nfe", ctypes.c_int64), ("nje", ctypes.c_int64), ("nlu", ctypes.c_int64),
+                ("netf", ctypes.c_int64), ("ncfn", ctypes.c_int64), ("max_nfe", ctypes.c_int32),
+                ("max_nst", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class B200ChemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"b200chem error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: os.PathLike | None = None):
+    """Load libb200chem.so (raises if it is missing: no fallback exists)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else Path(os.environ.get("B200CHEM_LIB", LIB_PATH))
+    if not p.exists():
+        raise FileNotFoundError(f"{p} not built; run __graft_entry__.build() or python -m pelelmex_b200.build")
+    L = ctypes.CDLL(str(p))
+    from .mechanism import MechDesc
+    L.b200chem_version.restype = ctypes.c_int
+    L.b200chem_last_error.restype = ctypes.c_char_p
+    L.b200chem_create.restype = ctypes.c_void_p
+    L.b200chem_create.argtypes = [ctypes.POINTER(MechDesc), ctypes.POINTER(Opts)]
+    L.b200chem_set_typvals.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int32]
+    L.b200chem_react.argtypes = [ctypes.c_void_p, ctypes.POINTER(BoxView), ctypes.c_int32,
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_void_p,
+                                 ctypes.c_void_p, ctypes.POINTER(Stats)]
+    L.b200chem_react_flat.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_void_p,
+                                      ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.POINTER(Stats)]
+    L.b200chem_destroy.argtypes = [ctypes.c_void_p]
+    for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):
+        f = getattr(L, name)
+        f.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, _f64p, ctypes.c_void_p]
+    L.b200chem_inst_rr.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
+    L.b200chem_t_from_hy.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
+    for name in ("b200chem_set_typvals", "b200chem_react", "b200chem_react_flat", "b200chem_destroy",
+                 "b200chem_eval_rhs", "b200chem_eval_jac", "b200chem_inst_rr", "b200chem_t_from_hy"):
+        getattr(L, name).restype = ctypes.c_int
+    if path is None:
+        _lib = L
+    return L
+
+
+def check(code: int):
+    if code != 0:
+        raise B200ChemError(code, load().b200chem_last_error().decode())
+    return code

@@ -1,0 +1,72 @@
+"""Build the in-tree CUDA library libb200chem.so for sm_100a.
+
+    python -m pelelmex_b200.build [--force]
+
+nvcc cross-compiles without a GPU.  The library is rebuilt only when a
+source under csrc/ or include/ is newer than it.
+"""
+from __future__ import annotations
+
+import argparse
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+LIB = PKG / "libb200chem.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+              "--expt-relaxed-constexpr", "-diag-suppress", "128"]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def sources():
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> Path:
+    deps = list(CSRC.glob("*")) + list(INCLUDE.rglob("*.h")) + list(INCLUDE.rglob("*.H"))
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, sources()), "-I", str(INCLUDE)]
+    if ptxas_v:
+        cmd += ["-Xptxas", "-v"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libb200chem.so")
+    if verbose or ptxas_v:
+        sys.stderr.write(res.stderr)
+    return LIB
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=True, ptxas_v=a.ptxas_v))
+
+
+if __name__ == "__main__":
+    main()

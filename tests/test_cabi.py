@@ -1,0 +1,44 @@
+"""The C ABI library loads and exports every symbol include/b200chem.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared():
+    txt = (ROOT / "include" / "b200chem.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(b200chem_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    for n in ("b200chem_create", "b200chem_set_typvals", "b200chem_react", "b200chem_react_flat",
+              "b200chem_destroy", "b200chem_eval_rhs", "b200chem_eval_jac", "b200chem_inst_rr",
+              "b200chem_t_from_hy"):
+        assert n in names
+
+
+def test_library_exports_all_declared_symbols():
+    from pelelmex_b200 import build
+    lib = ctypes.CDLL(str(build.build()))
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.b200chem_version() == 1
+
+
+def test_struct_layouts_match_header():
+    from pelelmex_b200 import _lib
+    assert ctypes.sizeof(_lib.Array4) == 8 + 3 * 8 + 6 * 4
+    assert ctypes.sizeof(_lib.BoxView) == 24 + 7 * ctypes.sizeof(_lib.Array4)
+    assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 6 * 4
+
+
+def test_null_handle_is_rejected_without_gpu():
+    from pelelmex_b200 import _lib
+    L = _lib.load()
+    dt = ctypes.c_double(1e-6)
+    assert L.b200chem_react(None, None, 0, ctypes.byref(dt), None, None, None, None) == -1
+    assert b"bad arguments" in L.b200chem_last_error()
