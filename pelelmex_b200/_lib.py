@@ -19,7 +19,8 @@ _f64p = ctypes.c_void_p  # device pointers are passed as integers
 class Opts(ctypes.Structure):
     _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_order", ctypes.c_int32),
                 ("max_steps", ctypes.c_int32), ("reactor_type", ctypes.c_int32), ("lu_fp64", ctypes.c_int32),
-                ("warps_per_cta", ctypes.c_int32), ("verbose", ctypes.c_int32)]
+                ("warps_per_cta", ctypes.c_int32), ("verbose", ctypes.c_int32), ("kernel", ctypes.c_int32),
+                ("setup_ratio", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
 
 
 class Array4(ctypes.Structure):

@@ -15,7 +15,7 @@
 #include <vector>
 
 #include "../../include/b200chem.h"
-#include "bdf_warp.cuh"
+#include "bdf_thread.cuh"
 
 using namespace b200;
 
@@ -249,6 +249,204 @@ __global__ void __launch_bounds__(128, B200_REACT_MIN_CTAS) react_kernel(ReactPa
   }
 }
 
+// ------------------------------------------------ thread-per-cell kernel
+constexpr int kTpcBlock = 128;
+#ifndef B200_TPC_MIN_CTAS
+#define B200_TPC_MIN_CTAS 4
+#endif
+
+struct TpcParams {
+  double* J;        // [n*n][threads] FP64 Jacobians, interleaved by thread
+  void* A;          // [n*n][threads] LU factors (float or double), interleaved
+  long long nthr;   // threads in the launch (interleave stride)
+  int setup_ratio;  // setup round when waiting * ratio >= needing an RHS
+};
+
+__device__ __forceinline__ int find_box(const ReactParams& P, const long long* s_off, int nb_s, long long cell) {
+  int lo = 0, hi = P.nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long o = nb_s ? s_off[mid] : P.boxes[mid].off;
+    if (o <= cell) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int NS, typename LUT>
+__global__ void __launch_bounds__(kTpcBlock, B200_TPC_MIN_CTAS) react_tpc_kernel(ReactParams P, TpcParams Q) {
+  using namespace b200::tpc;
+  constexpr int n = NS + 1;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ DevMech s_mech;
+  __shared__ long long s_off[65];
+  if (threadIdx.x == 0) s_mech = P.mech;
+  const int nb_s = P.nbox <= 64 ? P.nbox : 0;
+  for (int b = threadIdx.x; b <= nb_s; b += blockDim.x) s_off[b] = (b < nb_s) ? P.boxes[b].off : P.total;
+  __syncthreads();
+  const DevMech& m = s_mech;
+  const int lane = threadIdx.x & 31;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double* sC = reinterpret_cast<double*>(dsm) + threadIdx.x;
+  double* sW = sC + NS * kTpcBlock;
+  const IMat<double> J{Q.J + gtid, Q.nthr, n};
+  const IMat<LUT> A{reinterpret_cast<LUT*>(Q.A) + gtid, Q.nthr, n};
+  double atolv[n];
+#pragma unroll
+  for (int i = 0; i < n; ++i) atolv[i] = P.atol[i];
+
+  Cell<NS, LUT> c;
+  int phase = kIdle;
+  long long cell = -1;
+  bool qdone = false;  // warp-uniform: the queue is exhausted
+  long long acc[kStCount];
+#pragma unroll
+  for (int i = 0; i < kStCount; ++i) acc[i] = 0;
+
+  for (long long round = 0;; ++round) {
+    // ---- refill idle threads from the global queue (warp-aggregated atomics)
+    for (;;) {
+      const unsigned idle = __ballot_sync(kFull, phase == kIdle);
+      if (idle == 0) break;
+      if (qdone) {
+        if (phase == kIdle) phase = kExhausted;
+        break;
+      }
+      const int leader = __ffs(idle) - 1;
+      const int cnt = __popc(idle);
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(P.queue, (unsigned long long)cnt);
+      base = __shfl_sync(kFull, base, leader);
+      if (base + cnt >= (unsigned long long)P.total) qdone = true;
+      if (phase == kIdle) {
+        const unsigned long long idx = base + __popc(idle & ((1u << lane) - 1u));
+        if (idx >= (unsigned long long)P.total) {
+          phase = kExhausted;
+        } else {
+          const long long cl = (long long)idx;
+          const DevBox& bx = P.boxes[find_box(P, s_off, nb_s, cl)];
+          const long long loc = cl - bx.off;
+          const int i = bx.lo0 + (int)(loc % bx.nx);
+          const int j = bx.lo1 + (int)((loc / bx.nx) % bx.ny);
+          const int k = bx.lo2 + (int)(loc / ((long long)bx.nx * bx.ny));
+          bool masked = false;
+          if (bx.mask.p)
+            masked = bx.mask.p[(long long)(i - bx.mask.lo0) + (long long)(j - bx.mask.lo1) * bx.mask.js +
+                               (long long)(k - bx.mask.lo2) * bx.mask.ks] == 0;
+          int code = 0;
+          if (masked) {
+            if (bx.fc.p) *elem(bx.fc, i, j, k) = 0.0;
+            acc[kStMasked]++;
+            code = B200CHEM_CELL_MASKED;
+          } else {
+            const double* yp = elem(bx.rhoY, i, j, k);
+            const double* fp = elem(bx.fY, i, j, k);
+            double rho = 0.0;
+            bool bad = false;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              c.zn[0][q] = yp[q * bx.rhoY.ns];
+              c.F[q] = fp[q * bx.fY.ns];
+              rho += c.zn[0][q];
+              bad |= !isfinite(c.zn[0][q]) || !isfinite(c.F[q]);
+            }
+            c.zn[0][NS] = *elem(bx.T, i, j, k);
+            c.F[NS] = *elem(bx.fH, i, j, k);
+            bad |= !(c.zn[0][NS] > 0.0) || !isfinite(c.zn[0][NS]) || !isfinite(c.F[NS]) || !(rho > 0.0);
+            if (bad) {
+              code = B200CHEM_CELL_NONFINITE;
+              if (bx.fc.p) *elem(bx.fc, i, j, k) = 0.0;
+              acc[kStCells]++;
+              acc[kStFailed]++;
+            } else {
+              cell = cl;
+              phase = c_begin<NS, LUT>(c, atolv, P.rtol, P.dt, P.qmax, P.max_steps);
+            }
+          }
+          if (phase == kIdle && P.status) P.status[cl] = code;
+        }
+      }
+    }
+    const unsigned live = __ballot_sync(kFull, phase != kExhausted);
+    if (live == 0) break;
+    // ---- one round: RHS for every cell that needs it, or Jacobian + LU
+    const unsigned nr = __ballot_sync(kFull, needs_rhs(phase));
+    const unsigned ns = __ballot_sync(kFull, phase == kSetup);
+    const bool setup_round = ns != 0 && (nr == 0 || __popc(ns) * Q.setup_ratio >= __popc(nr));
+    int status = 0;
+    if (setup_round) {
+      if (phase == kSetup) {
+        const int ier = c_setup<NS, LUT>(c, m, J, A, sC, sW, kTpcBlock);
+        phase = c_advance<NS, LUT>(c, kLAfterSetup, nullptr, ier, atolv, P.rtol, J, A, &status);
+      }
+    } else if (needs_rhs(phase)) {
+      double f[n];
+      tpc_rhs<NS>(m, c.yev, c.F, f, sC, sW, kTpcBlock);
+      c.cnt.nfe++;
+      const int lab = (phase == kRhsF0) ? kLAfterF0
+                      : (phase == kRhsHin) ? kLAfterHin
+                      : (phase == kRhsNStart) ? kLAfterNStart
+                      : (phase == kRhsNIter) ? kLAfterNIter : kLAfterRestart;
+      phase = c_advance<NS, LUT>(c, lab, f, 0, atolv, P.rtol, J, A, &status);
+    }
+    // ---- finished cells: write back and account
+    if (phase == kIdle && cell >= 0) {
+      const DevBox& bx = P.boxes[find_box(P, s_off, nb_s, cell)];
+      const long long loc = cell - bx.off;
+      const int i = bx.lo0 + (int)(loc % bx.nx);
+      const int j = bx.lo1 + (int)((loc / bx.nx) % bx.ny);
+      const int k = bx.lo2 + (int)(loc / ((long long)bx.nx * bx.ny));
+      if (status == 0) {
+        // y(dt) from the Nordsieck array (Horner in s = (dt - tn)/h)
+        const double s = (P.dt - c.tn) / c.h;
+        double* yp = elem(bx.rhoY, i, j, k);
+#pragma unroll
+        for (int q = 0; q < n; ++q) {
+          double v = c.zn[c.q][q];
+          for (int jj = c.q - 1; jj >= 0; --jj) v = c.zn[jj][q] + s * v;
+          if (q < NS) yp[q * bx.rhoY.ns] = v;
+          else *elem(bx.T, i, j, k) = v;
+        }
+        double* hp = elem(bx.rhoH, i, j, k);
+        *hp = *hp + P.dt * c.F[NS];
+      } else {
+        acc[kStFailed]++;
+      }
+      if (bx.fc.p) *elem(bx.fc, i, j, k) = (double)c.cnt.nfe;
+      if (P.status) P.status[cell] = status;
+      acc[kStCells]++;
+      acc[kStNst] += c.cnt.nst;
+      acc[kStNfe] += c.cnt.nfe;
+      acc[kStNje] += c.cnt.nje;
+      acc[kStNlu] += c.cnt.nlu;
+      acc[kStNetf] += c.cnt.netf;
+      acc[kStNcfn] += c.cnt.ncfn;
+      acc[kStMaxNfe] = max(acc[kStMaxNfe], (long long)c.cnt.nfe);
+      acc[kStMaxNst] = max(acc[kStMaxNst], (long long)c.cnt.nst);
+      cell = -1;
+    }
+  }
+  if (P.stats) {
+#pragma unroll
+    for (int s = 0; s < kStMaxNfe; ++s) {
+      long long v = acc[s];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+      if (lane == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(P.stats + s), (unsigned long long)v);
+    }
+    long long mx = acc[kStMaxNfe], ms = acc[kStMaxNst];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+      ms = max(ms, __shfl_xor_sync(kFull, ms, o));
+    }
+    if (lane == 0) {
+      atomicMax(P.stats + kStMaxNfe, mx);
+      atomicMax(P.stats + kStMaxNst, ms);
+    }
+  }
+}
+
 // ------------------------------------------------ evaluation-only kernels
 struct EvalParams {
   DevMech mech;
@@ -399,6 +597,8 @@ struct b200chem_reactor {
   int sm_count = 0;
   int Npad = 32, Rpad = 32, ldj = 0, ldl = 0;
   int warps_per_cta = 4;
+  void* d_tpc = nullptr;  // thread-per-cell scratch (Jacobians + LU factors)
+  size_t tpc_bytes = 0;
 };
 
 namespace {
@@ -452,6 +652,54 @@ int launch_react(b200chem_reactor* h, const ReactParams& P, int warps, cudaStrea
   return 0;
 }
 
+bool tpc_supported(int N) { return N == 9 || N == 21; }
+
+template <int NS, typename LUT>
+int launch_tpc(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+  const int n = NS + 1;
+  const int smem = (int)(2 * sizeof(double) * NS * kTpcBlock);
+  CK(cudaFuncSetAttribute(react_tpc_kernel<NS, LUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, react_tpc_kernel<NS, LUT>, kTpcBlock, smem));
+  if (per_sm < 1) return set_err(B200CHEM_ETOOBIG, "thread-per-cell kernel does not fit on an SM");
+  if (h->opts.ctas_per_sm > 0) per_sm = std::min(per_sm, (int)h->opts.ctas_per_sm);
+  long long need = (P.total + kTpcBlock - 1) / kTpcBlock;
+  long long grid = std::min<long long>(need, (long long)h->sm_count * per_sm);
+  if (grid < 1) grid = 1;
+  const long long nthr = grid * kTpcBlock;
+  const size_t bytes = (size_t)nthr * n * n * (sizeof(double) + sizeof(LUT));
+  if (bytes > h->tpc_bytes) {
+    if (h->d_tpc) {
+      CK(cudaStreamSynchronize(st));
+      cudaFree(h->d_tpc);
+      h->d_tpc = nullptr;
+      h->tpc_bytes = 0;
+    }
+    if (cudaMalloc(&h->d_tpc, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(B200CHEM_ENOMEM, "cannot allocate %zu bytes of integrator scratch", bytes);
+    }
+    h->tpc_bytes = bytes;
+  }
+  TpcParams Q;
+  Q.J = static_cast<double*>(h->d_tpc);
+  Q.A = static_cast<void*>(static_cast<double*>(h->d_tpc) + (size_t)nthr * n * n);
+  Q.nthr = nthr;
+  Q.setup_ratio = h->opts.setup_ratio > 0 ? h->opts.setup_ratio : 2;
+  react_tpc_kernel<NS, LUT><<<(unsigned)grid, kTpcBlock, smem, st>>>(P, Q);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename LUT>
+int launch_tpc_n(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+  switch (h->N) {
+    case 9: return launch_tpc<9, LUT>(h, P, st);
+    case 21: return launch_tpc<21, LUT>(h, P, st);
+    default: return set_err(B200CHEM_EINVAL, "no thread-per-cell variant for N=%d", h->N);
+  }
+}
+
 int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long total, double dt, cudaStream_t st,
              int32_t* cell_status, b200chem_stats* stats) {
   const int nbox = (int)boxes.size();
@@ -492,8 +740,12 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   P.warp_bytes = smem_warp_bytes(h, fp64);
   const int warps = fit_warps(P.warp_bytes, h->opts.warps_per_cta > 0 ? h->opts.warps_per_cta : h->warps_per_cta);
   int err;
+  const bool use_tpc = (h->opts.kernel == 1) || (h->opts.kernel == 0 && tpc_supported(h->N));
+  if (h->opts.kernel == 1 && !tpc_supported(h->N))
+    return set_err(B200CHEM_EINVAL, "thread-per-cell kernel requested but not compiled for N=%d", h->N);
   if (total > 0) {
-    if (h->cpl == 1) err = fp64 ? launch_react<1, double>(h, P, warps, st) : launch_react<1, float>(h, P, warps, st);
+    if (use_tpc) err = fp64 ? launch_tpc_n<double>(h, P, st) : launch_tpc_n<float>(h, P, st);
+    else if (h->cpl == 1) err = fp64 ? launch_react<1, double>(h, P, warps, st) : launch_react<1, float>(h, P, warps, st);
     else err = fp64 ? launch_react<2, double>(h, P, warps, st) : launch_react<2, float>(h, P, warps, st);
     if (err) return err;
   }
@@ -786,6 +1038,7 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->d_scratch) cudaFree(h->d_scratch);
   if (h->d_boxes) cudaFree(h->d_boxes);
   if (h->h_boxes) cudaFreeHost(h->h_boxes);
+  if (h->d_tpc) cudaFree(h->d_tpc);
   delete h;
   return 0;
 }

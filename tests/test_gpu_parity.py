@@ -38,9 +38,9 @@ def _dev(a, dtype=torch.float64):
 
 
 def run_gpu(name, f, rtol=1e-8, atol=1e-12, max_order=5, lu_fp64=False, typ=None, mask=None, max_steps=10000,
-            fY=None, fH=None):
+            fY=None, fH=None, kernel="auto"):
     r = ReactorB200(name, rtol=rtol, atol=atol, max_order=max_order, lu_fp64=lu_fp64,
-                    max_steps=max_steps).init(2, f.ncells)
+                    max_steps=max_steps, kernel=kernel).init(2, f.ncells)
     if typ is not None:
         r.set_typ_vals_ode(typ)
     rhoY, T, rhoH = _dev(f.rhoY), _dev(f.T), _dev(f.rhoH)
@@ -144,6 +144,19 @@ def test_dodecane_two_components_per_lane(orc_cache):
     print(f"dodecane-shaped: T err vs oracle {terr.max():.2e}; Y err vs rtol-1e-12 solve: gpu {eg.max():.2e} "
           f"oracle {eo.max():.2e}")
     assert eg.max() <= 3.0 * eo.max() + 1e-9
+
+
+@pytest.mark.parametrize("kernel", ["warp", "thread"])
+@pytest.mark.parametrize("lu_fp64", [False, True])
+def test_both_kernels_and_lu_precisions(kernel, lu_fp64, orc_cache):
+    """Thread-per-cell and warp-per-cell kernels, FP32+refinement and FP64 LU."""
+    mech = M.builtin("synth_ch4_21")
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 1024, seed=13), dt=1e-5)
+    g = run_gpu("synth_ch4_21", f, kernel=kernel, lu_fp64=lu_fp64)
+    o = orc_cache("synth_ch4_21").react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12,
+                                        max_order=5)
+    assert (g["status"] == 0).all()
+    compare(f, g, o, f"{kernel} kernel, lu_fp64={lu_fp64}")
 
 
 def test_fp64_lu_variant(orc_cache):
