@@ -90,16 +90,18 @@ typedef struct b200chem_opts {
   int32_t max_steps;     /* maximum internal steps per cell and call            */
   int32_t reactor_type;  /* 2 = HP (constant pressure, enthalpy forcing); only 2 */
   int32_t lu_fp64;       /* 0: FP32 LU + one FP64 refinement step (default); 1: FP64 LU */
-  int32_t warps_per_cta; /* 0: use the autotuned / default launch shape         */
+  int32_t warps_per_cta; /* unused; kept for layout stability (set 0)           */
   int32_t verbose;
-  int32_t kernel;        /* 0: auto (thread-per-cell when the species count has a
-                            compiled variant, else warp-per-cell); 1: thread-per-
-                            cell; 2: warp-per-cell                                */
+  int32_t kernel;        /* 0: auto (group integrator); 1: thread-per-cell (only
+                            species counts with a compiled variant); 2: group
+                            integrator                                           */
   int32_t setup_ratio;   /* thread-per-cell: a warp runs a Jacobian/LU round when
                             (cells waiting) * setup_ratio >= (cells needing an
                             RHS); 0 = default (2)                                */
-  int32_t ctas_per_sm;   /* thread-per-cell: resident CTAs per SM (0 = as many as
-                            fit); fewer keeps the per-cell state in L2         */
+  int32_t ctas_per_sm;   /* resident CTAs per SM (0 = as many as fit); fewer
+                            keeps the per-cell scratch in L2                  */
+  int32_t group_lanes;   /* group integrator: lanes per cell, 8, 16 or 32
+                            (0 = default for the mechanism size)              */
 } b200chem_opts;
 
 /* ---------------------------------------------------------- Array4 views

@@ -20,7 +20,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_order", ctypes.c_int32),
                 ("max_steps", ctypes.c_int32), ("reactor_type", ctypes.c_int32), ("lu_fp64", ctypes.c_int32),
                 ("warps_per_cta", ctypes.c_int32), ("verbose", ctypes.c_int32), ("kernel", ctypes.c_int32),
-                ("setup_ratio", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+                ("setup_ratio", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("group_lanes", ctypes.c_int32)]
 
 
 class Array4(ctypes.Structure):

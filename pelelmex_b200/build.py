@@ -42,21 +42,42 @@ def _stale(target: Path, deps) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> Path:
+def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False, jobs: int = 0) -> Path:
+    """Compile every csrc/*.cu to an object in parallel, then link libb200chem.so."""
+    import concurrent.futures as cf
+    import os
+
     deps = list(CSRC.glob("*")) + list(INCLUDE.rglob("*.h")) + list(INCLUDE.rglob("*.H"))
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, sources()), "-I", str(INCLUDE)]
-    if ptxas_v:
-        cmd += ["-Xptxas", "-v"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    srcs = sources()
+
+    def compile_one(src: Path):
+        obj = objdir / (src.stem + ".o")
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", "-o", str(obj), str(src), "-I", str(INCLUDE)]
+        if ptxas_v:
+            cmd += ["-Xptxas", "-v"]
+        return src, obj, cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+    jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    objs, logs = [], []
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        for src, obj, cmd, res in ex.map(compile_one, srcs):
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            if res.returncode != 0:
+                sys.stderr.write(res.stdout + res.stderr)
+                raise RuntimeError(f"nvcc failed on {src.name}")
+            logs.append(res.stderr)
+            objs.append(str(obj))
+    res = subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *objs], capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libb200chem.so")
+        raise RuntimeError("linking libb200chem.so failed")
     if verbose or ptxas_v:
-        sys.stderr.write(res.stderr)
+        sys.stderr.write("".join(logs))
     return LIB
 
 

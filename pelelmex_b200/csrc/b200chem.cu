@@ -1,10 +1,7 @@
-// b200chem.cu -- kernels and C ABI of the B200 HP chemistry reactor.
-//
-// One persistent launch advances every cell of a list of boxes: each warp
-// takes cells from a global atomic queue (work stealing, so cells that need
-// thousands of BDF steps do not hold back cells that need a handful) and
-// integrates one cell at a time with WarpBdf (bdf_warp.cuh).  The launch is
-// sized to fill the GPU exactly once (SM count x resident CTAs per SM).
+// b200chem.cu -- C ABI and host side of the B200 HP chemistry reactor, plus
+// the mechanism-evaluation kernels (RHS, Jacobian, instantaneous rates,
+// T from (h, Y)).  The react kernels live in react_g*.cu (group integrator)
+// and react_tpc.cu (thread-per-cell integrator).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,8 +11,8 @@
 #include <string>
 #include <vector>
 
-#include "../../include/b200chem.h"
-#include "bdf_thread.cuh"
+#include "common.cuh"
+#include "react_group.cuh"
 
 using namespace b200;
 
@@ -33,429 +30,22 @@ int set_err(int code, const char* fmt, ...) {
   return code;
 }
 
-#define CK(x)                                                                              \
-  do {                                                                                     \
-    cudaError_t e_ = (x);                                                                  \
+#define CK(x)                                                                                     \
+  do {                                                                                            \
+    cudaError_t e_ = (x);                                                                         \
     if (e_ != cudaSuccess) return set_err(B200CHEM_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
   } while (0)
 
-struct DevArr {
-  double* p;
-  long long js, ks, ns;
-  int lo0, lo1, lo2, pad;
-};
-struct DevIArr {
-  const int* p;
-  long long js, ks;
-  int lo0, lo1, lo2, pad;
-};
-struct DevBox {
-  int lo0, lo1, lo2, nx, ny, nz;
-  long long off;
-  DevArr rhoY, fY, T, rhoH, fH, fc;
-  DevIArr mask;
-};
-
-// stats slots in the scratch buffer (after the queue counter)
-enum { kStCells = 0, kStMasked, kStFailed, kStNst, kStNfe, kStNje, kStNlu, kStNetf, kStNcfn, kStMaxNfe,
-       kStMaxNst, kStCount };
-
-struct ReactParams {
-  DevMech mech;
-  const DevBox* boxes;
-  int nbox;
-  long long total;
-  double dt;
-  int max_steps;
-  int qmax;
-  double rtol;
-  const double* atol;
-  unsigned long long* queue;
-  long long* stats;
-  int* status;
-  int warp_bytes;
-  int Npad, Rpad, ldj, ldl;
-};
-
-__device__ __forceinline__ double* elem(const DevArr& a, int i, int j, int k) {
-  return a.p + (long long)(i - a.lo0) + (long long)(j - a.lo1) * a.js + (long long)(k - a.lo2) * a.ks;
-}
-
-template <int CPL, typename LUT>
-__device__ __forceinline__ void carve(WarpBdf<CPL, LUT>& B, unsigned char* base, int n, int Npad, int Rpad, int ldj,
-                                      int ldl) {
-  double* d = reinterpret_cast<double*>(base);
-  B.ms.C = d;
-  d += Npad;
-  B.ms.gRT = d;
-  d += Npad;
-  B.ms.hRT = d;
-  d += Npad;
-  B.ms.r0 = d;
-  d += Rpad;
-  B.ms.r1 = d;
-  d += Rpad;
-  B.ms.r2 = d;
-  d += Rpad;
-  B.ms.r3 = d;
-  d += Rpad;
-  B.ms.r4 = d;
-  d += Rpad;
-  B.atolv = d;
-  d += Npad;
-  B.Dsc = d;
-  d += Npad;
-  B.J = d;
-  d += (size_t)n * ldj;
-  B.LU = reinterpret_cast<LUT*>(d);
-  B.perm = reinterpret_cast<int*>(B.LU + (size_t)n * ldl);
-  B.ldj = ldj;
-  B.ldl = ldl;
-}
-
-// Minimum resident CTAs per SM requested from the compiler (register budget):
-// 1 lets the integrator keep all of its state in registers (up to 255).
-#ifndef B200_REACT_MIN_CTAS
-#define B200_REACT_MIN_CTAS 1
-#endif
-
-template <int CPL, typename LUT>
-__global__ void __launch_bounds__(128, B200_REACT_MIN_CTAS) react_kernel(ReactParams P) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  __shared__ DevMech s_mech;
-  __shared__ long long s_off[65];
-  if (threadIdx.x == 0) s_mech = P.mech;
-  const int nb_s = P.nbox <= 64 ? P.nbox : 0;
-  for (int b = threadIdx.x; b <= nb_s; b += blockDim.x) s_off[b] = (b < nb_s) ? P.boxes[b].off : P.total;
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
-  const int N = P.mech.N, n = N + 1;
-
-  WarpBdf<CPL, LUT> B;
-  B.m = &s_mech;
-  B.lane = lane;
-  B.n = n;
-  B.qmax = P.qmax;
-  B.rtol = P.rtol;
-  carve<CPL, LUT>(B, dsm + (size_t)w * P.warp_bytes, n, P.Npad, P.Rpad, P.ldj, P.ldl);
-  for (int k = lane; k < n; k += 32) B.atolv[k] = P.atol[k];
-  __syncwarp();
-  long long acc[kStCount];
-#pragma unroll
-  for (int i = 0; i < kStCount; ++i) acc[i] = 0;
-
-  for (;;) {
-    unsigned long long cell = 0;
-    if (lane == 0) cell = atomicAdd(P.queue, 1ull);
-    cell = __shfl_sync(kFull, cell, 0);
-    if (cell >= (unsigned long long)P.total) break;
-    // locate the box (offsets are increasing)
-    int lo = 0, hi = P.nbox - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      const long long o = nb_s ? s_off[mid] : P.boxes[mid].off;
-      if (o <= (long long)cell) lo = mid;
-      else hi = mid - 1;
-    }
-    const DevBox& bx = P.boxes[lo];
-    const long long loc = (long long)cell - bx.off;
-    const int i = bx.lo0 + (int)(loc % bx.nx);
-    const int j = bx.lo1 + (int)((loc / bx.nx) % bx.ny);
-    const int k = bx.lo2 + (int)(loc / ((long long)bx.nx * bx.ny));
-    int code;
-    double* fcp = bx.fc.p ? elem(bx.fc, i, j, k) : nullptr;
-    bool masked = false;
-    if (bx.mask.p) {
-      const int mv = bx.mask.p[(long long)(i - bx.mask.lo0) + (long long)(j - bx.mask.lo1) * bx.mask.js +
-                               (long long)(k - bx.mask.lo2) * bx.mask.ks];
-      masked = (mv == 0);
-    }
-    if (masked) {
-      code = B200CHEM_CELL_MASKED;
-      if (lane == 0) {
-        if (fcp) *fcp = 0.0;
-        acc[kStMasked]++;
-      }
-    } else {
-      double* yp = elem(bx.rhoY, i, j, k);
-      double* fp = elem(bx.fY, i, j, k);
-      double* tp = elem(bx.T, i, j, k);
-      double yv[CPL], fv[CPL];
-      double rho = 0.0;
-      bool bad = false;
-#pragma unroll
-      for (int c = 0; c < CPL; ++c) {
-        const int q = lane + 32 * c;
-        yv[c] = 0.0;
-        fv[c] = 0.0;
-        if (q < N) {
-          yv[c] = yp[q * bx.rhoY.ns];
-          fv[c] = fp[q * bx.fY.ns];
-          rho += yv[c];
-        } else if (q == N) {
-          yv[c] = *tp;
-          fv[c] = *elem(bx.fH, i, j, k);
-          bad |= !(yv[c] > 0.0);
-        }
-        bad |= !isfinite(yv[c]) || !isfinite(fv[c]);
-      }
-      rho = warp_sum(rho);
-      bad |= !(rho > 0.0);
-      if (__any_sync(kFull, bad)) {
-        code = B200CHEM_CELL_NONFINITE;
-        B.cnt = CellCounters{0, 0, 0, 0, 0, 0, 0};
-      } else {
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) B.F[c] = fv[c];
-        code = B.integrate(yv, P.dt, P.max_steps);
-      }
-      double fh = 0.0;
-      if (lane == 0) fh = *elem(bx.fH, i, j, k);
-      if (code == 0) {
-#pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int q = lane + 32 * c;
-          if (q < N) yp[q * bx.rhoY.ns] = yv[c];
-          else if (q == N) *tp = yv[c];
-        }
-        if (lane == 0) {
-          double* hp = elem(bx.rhoH, i, j, k);
-          *hp = *hp + P.dt * fh;
-        }
-      }
-      if (lane == 0) {
-        if (fcp) *fcp = (double)B.cnt.nfe;
-        acc[kStCells]++;
-        if (code != 0) acc[kStFailed]++;
-        acc[kStNst] += B.cnt.nst;
-        acc[kStNfe] += B.cnt.nfe;
-        acc[kStNje] += B.cnt.nje;
-        acc[kStNlu] += B.cnt.nlu;
-        acc[kStNetf] += B.cnt.netf;
-        acc[kStNcfn] += B.cnt.ncfn;
-        acc[kStMaxNfe] = max(acc[kStMaxNfe], (long long)B.cnt.nfe);
-        acc[kStMaxNst] = max(acc[kStMaxNst], (long long)B.cnt.nst);
-      }
-    }
-    if (lane == 0 && P.status) P.status[cell] = code;
-  }
-  if (lane == 0 && P.stats) {
-#pragma unroll
-    for (int s = 0; s < kStMaxNfe; ++s)
-      if (acc[s]) atomicAdd(reinterpret_cast<unsigned long long*>(P.stats + s), (unsigned long long)acc[s]);
-    atomicMax(P.stats + kStMaxNfe, acc[kStMaxNfe]);
-    atomicMax(P.stats + kStMaxNst, acc[kStMaxNst]);
-  }
-}
-
-// ------------------------------------------------ thread-per-cell kernel
-constexpr int kTpcBlock = 128;
-#ifndef B200_TPC_MIN_CTAS
-#define B200_TPC_MIN_CTAS 4
-#endif
-
-struct TpcParams {
-  double* J;        // [n*n][threads] FP64 Jacobians, interleaved by thread
-  void* A;          // [n*n][threads] LU factors (float or double), interleaved
-  long long nthr;   // threads in the launch (interleave stride)
-  int setup_ratio;  // setup round when waiting * ratio >= needing an RHS
-};
-
-__device__ __forceinline__ int find_box(const ReactParams& P, const long long* s_off, int nb_s, long long cell) {
-  int lo = 0, hi = P.nbox - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    const long long o = nb_s ? s_off[mid] : P.boxes[mid].off;
-    if (o <= cell) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-template <int NS, typename LUT>
-__global__ void __launch_bounds__(kTpcBlock, B200_TPC_MIN_CTAS) react_tpc_kernel(ReactParams P, TpcParams Q) {
-  using namespace b200::tpc;
-  constexpr int n = NS + 1;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  __shared__ DevMech s_mech;
-  __shared__ long long s_off[65];
-  if (threadIdx.x == 0) s_mech = P.mech;
-  const int nb_s = P.nbox <= 64 ? P.nbox : 0;
-  for (int b = threadIdx.x; b <= nb_s; b += blockDim.x) s_off[b] = (b < nb_s) ? P.boxes[b].off : P.total;
-  __syncthreads();
-  const DevMech& m = s_mech;
-  const int lane = threadIdx.x & 31;
-  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double* sC = reinterpret_cast<double*>(dsm) + threadIdx.x;
-  double* sW = sC + NS * kTpcBlock;
-  const IMat<double> J{Q.J + gtid, Q.nthr, n};
-  const IMat<LUT> A{reinterpret_cast<LUT*>(Q.A) + gtid, Q.nthr, n};
-  double atolv[n];
-#pragma unroll
-  for (int i = 0; i < n; ++i) atolv[i] = P.atol[i];
-
-  Cell<NS, LUT> c;
-  int phase = kIdle;
-  long long cell = -1;
-  bool qdone = false;  // warp-uniform: the queue is exhausted
-  long long acc[kStCount];
-#pragma unroll
-  for (int i = 0; i < kStCount; ++i) acc[i] = 0;
-
-  for (long long round = 0;; ++round) {
-    // ---- refill idle threads from the global queue (warp-aggregated atomics)
-    for (;;) {
-      const unsigned idle = __ballot_sync(kFull, phase == kIdle);
-      if (idle == 0) break;
-      if (qdone) {
-        if (phase == kIdle) phase = kExhausted;
-        break;
-      }
-      const int leader = __ffs(idle) - 1;
-      const int cnt = __popc(idle);
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(P.queue, (unsigned long long)cnt);
-      base = __shfl_sync(kFull, base, leader);
-      if (base + cnt >= (unsigned long long)P.total) qdone = true;
-      if (phase == kIdle) {
-        const unsigned long long idx = base + __popc(idle & ((1u << lane) - 1u));
-        if (idx >= (unsigned long long)P.total) {
-          phase = kExhausted;
-        } else {
-          const long long cl = (long long)idx;
-          const DevBox& bx = P.boxes[find_box(P, s_off, nb_s, cl)];
-          const long long loc = cl - bx.off;
-          const int i = bx.lo0 + (int)(loc % bx.nx);
-          const int j = bx.lo1 + (int)((loc / bx.nx) % bx.ny);
-          const int k = bx.lo2 + (int)(loc / ((long long)bx.nx * bx.ny));
-          bool masked = false;
-          if (bx.mask.p)
-            masked = bx.mask.p[(long long)(i - bx.mask.lo0) + (long long)(j - bx.mask.lo1) * bx.mask.js +
-                               (long long)(k - bx.mask.lo2) * bx.mask.ks] == 0;
-          int code = 0;
-          if (masked) {
-            if (bx.fc.p) *elem(bx.fc, i, j, k) = 0.0;
-            acc[kStMasked]++;
-            code = B200CHEM_CELL_MASKED;
-          } else {
-            const double* yp = elem(bx.rhoY, i, j, k);
-            const double* fp = elem(bx.fY, i, j, k);
-            double rho = 0.0;
-            bool bad = false;
-#pragma unroll
-            for (int q = 0; q < NS; ++q) {
-              c.zn[0][q] = yp[q * bx.rhoY.ns];
-              c.F[q] = fp[q * bx.fY.ns];
-              rho += c.zn[0][q];
-              bad |= !isfinite(c.zn[0][q]) || !isfinite(c.F[q]);
-            }
-            c.zn[0][NS] = *elem(bx.T, i, j, k);
-            c.F[NS] = *elem(bx.fH, i, j, k);
-            bad |= !(c.zn[0][NS] > 0.0) || !isfinite(c.zn[0][NS]) || !isfinite(c.F[NS]) || !(rho > 0.0);
-            if (bad) {
-              code = B200CHEM_CELL_NONFINITE;
-              if (bx.fc.p) *elem(bx.fc, i, j, k) = 0.0;
-              acc[kStCells]++;
-              acc[kStFailed]++;
-            } else {
-              cell = cl;
-              phase = c_begin<NS, LUT>(c, atolv, P.rtol, P.dt, P.qmax, P.max_steps);
-            }
-          }
-          if (phase == kIdle && P.status) P.status[cl] = code;
-        }
-      }
-    }
-    const unsigned live = __ballot_sync(kFull, phase != kExhausted);
-    if (live == 0) break;
-    // ---- one round: RHS for every cell that needs it, or Jacobian + LU
-    const unsigned nr = __ballot_sync(kFull, needs_rhs(phase));
-    const unsigned ns = __ballot_sync(kFull, phase == kSetup);
-    const bool setup_round = ns != 0 && (nr == 0 || __popc(ns) * Q.setup_ratio >= __popc(nr));
-    int status = 0;
-    if (setup_round) {
-      if (phase == kSetup) {
-        const int ier = c_setup<NS, LUT>(c, m, J, A, sC, sW, kTpcBlock);
-        phase = c_advance<NS, LUT>(c, kLAfterSetup, nullptr, ier, atolv, P.rtol, J, A, &status);
-      }
-    } else if (needs_rhs(phase)) {
-      double f[n];
-      tpc_rhs<NS>(m, c.yev, c.F, f, sC, sW, kTpcBlock);
-      c.cnt.nfe++;
-      const int lab = (phase == kRhsF0) ? kLAfterF0
-                      : (phase == kRhsHin) ? kLAfterHin
-                      : (phase == kRhsNStart) ? kLAfterNStart
-                      : (phase == kRhsNIter) ? kLAfterNIter : kLAfterRestart;
-      phase = c_advance<NS, LUT>(c, lab, f, 0, atolv, P.rtol, J, A, &status);
-    }
-    // ---- finished cells: write back and account
-    if (phase == kIdle && cell >= 0) {
-      const DevBox& bx = P.boxes[find_box(P, s_off, nb_s, cell)];
-      const long long loc = cell - bx.off;
-      const int i = bx.lo0 + (int)(loc % bx.nx);
-      const int j = bx.lo1 + (int)((loc / bx.nx) % bx.ny);
-      const int k = bx.lo2 + (int)(loc / ((long long)bx.nx * bx.ny));
-      if (status == 0) {
-        // y(dt) from the Nordsieck array (Horner in s = (dt - tn)/h)
-        const double s = (P.dt - c.tn) / c.h;
-        double* yp = elem(bx.rhoY, i, j, k);
-#pragma unroll
-        for (int q = 0; q < n; ++q) {
-          double v = c.zn[c.q][q];
-          for (int jj = c.q - 1; jj >= 0; --jj) v = c.zn[jj][q] + s * v;
-          if (q < NS) yp[q * bx.rhoY.ns] = v;
-          else *elem(bx.T, i, j, k) = v;
-        }
-        double* hp = elem(bx.rhoH, i, j, k);
-        *hp = *hp + P.dt * c.F[NS];
-      } else {
-        acc[kStFailed]++;
-      }
-      if (bx.fc.p) *elem(bx.fc, i, j, k) = (double)c.cnt.nfe;
-      if (P.status) P.status[cell] = status;
-      acc[kStCells]++;
-      acc[kStNst] += c.cnt.nst;
-      acc[kStNfe] += c.cnt.nfe;
-      acc[kStNje] += c.cnt.nje;
-      acc[kStNlu] += c.cnt.nlu;
-      acc[kStNetf] += c.cnt.netf;
-      acc[kStNcfn] += c.cnt.ncfn;
-      acc[kStMaxNfe] = max(acc[kStMaxNfe], (long long)c.cnt.nfe);
-      acc[kStMaxNst] = max(acc[kStMaxNst], (long long)c.cnt.nst);
-      cell = -1;
-    }
-  }
-  if (P.stats) {
-#pragma unroll
-    for (int s = 0; s < kStMaxNfe; ++s) {
-      long long v = acc[s];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-      if (lane == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(P.stats + s), (unsigned long long)v);
-    }
-    long long mx = acc[kStMaxNfe], ms = acc[kStMaxNst];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mx = max(mx, __shfl_xor_sync(kFull, mx, o));
-      ms = max(ms, __shfl_xor_sync(kFull, ms, o));
-    }
-    if (lane == 0) {
-      atomicMax(P.stats + kStMaxNfe, mx);
-      atomicMax(P.stats + kStMaxNst, ms);
-    }
-  }
-}
-
 // ------------------------------------------------ evaluation-only kernels
+// One group of 32 lanes per cell (the mechanism functions of group_mech.cuh).
 struct EvalParams {
   DevMech mech;
   const double* y;
   const double* F;
   double* out;
   long long ncells;
-  int warp_bytes;
-  int Npad, Rpad, ldj, ldl;
+  GroupLayout L;
+  unsigned char* gscratch;
   int what;  // 0 rhs, 1 jac
 };
 
@@ -467,28 +57,32 @@ __global__ void __launch_bounds__(128) eval_kernel(EvalParams P) {
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int N = P.mech.N, n = N + 1;
-  WarpBdf<CPL, double> B;
-  carve<CPL, double>(B, dsm + (size_t)w * P.warp_bytes, n, P.Npad, P.Rpad, P.ldj, P.ldl);
+  GroupBdf<32, CPL, double> B;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
+  carve_group<32, CPL, double>(B, P.L, dsm + (size_t)w * P.L.smem_bytes, P.gscratch + gw * P.L.gbytes);
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long c0 = (long long)blockIdx.x * (blockDim.x >> 5) + w; c0 < P.ncells; c0 += wstride) {
-    double y[CPL], F[CPL], yd[CPL];
+  for (long long c0 = gw; c0 < P.ncells; c0 += wstride) {
+    Vec<CPL> y, F;
 #pragma unroll
     for (int c = 0; c < CPL; ++c) {
       const int q = lane + 32 * c;
-      y[c] = (q < n) ? P.y[c0 * n + q] : 0.0;
-      F[c] = (q < n) ? P.F[c0 * n + q] : 0.0;
+      y.v[c] = (q < n) ? P.y[c0 * n + q] : 0.0;
+      F.v[c] = (q < n) ? P.F[c0 * n + q] : 0.0;
     }
+    const Vec<CPL> yd = grp_rhs<32, CPL>(&s_mech, B.ms, y, F, lane);
     if (P.what == 0) {
-      warp_rhs<CPL>(s_mech, B.ms, y, F, yd, lane);
 #pragma unroll
       for (int c = 0; c < CPL; ++c)
-        if (lane + 32 * c < n) P.out[c0 * n + lane + 32 * c] = yd[c];
+        if (lane + 32 * c < n) P.out[c0 * n + lane + 32 * c] = yd.v[c];
     } else {
-      warp_jac<CPL>(s_mech, B.ms, y, F, yd, B.J, B.ldj, lane);
-      for (int i = 0; i < n; ++i)
+      grp_jac<32, CPL>(&s_mech, B.ms, y, yd, B.J, B.ldj, lane);
+      // B.J is column-major: (row i, col l) at l*ldj + i; the output is row-major
 #pragma unroll
-        for (int c = 0; c < CPL; ++c)
-          if (lane + 32 * c < n) P.out[(c0 * n + i) * n + lane + 32 * c] = B.J[i * B.ldj + lane + 32 * c];
+      for (int c = 0; c < CPL; ++c) {
+        const int l = lane + 32 * c;
+        if (l < n)
+          for (int i = 0; i < n; ++i) P.out[(c0 * n + i) * n + l] = B.J[l * B.ldj + i];
+      }
     }
     __syncwarp();
   }
@@ -497,6 +91,7 @@ __global__ void __launch_bounds__(128) eval_kernel(EvalParams P) {
 // T from (h, Y) by Newton on h(T) = sum Y_k h_k(T), warp per cell (HY2T).
 template <int CPL>
 __device__ double warp_t_from_hy(const DevMech& m, const double (&Y)[CPL], double h, double T, int lane) {
+  const Grp<32> g(lane);
   for (int it = 0; it < 100; ++it) {
     const double lnT = log(T);
     double hs = 0.0, cs = 0.0;
@@ -511,8 +106,8 @@ __device__ double warp_t_from_hy(const DevMech& m, const double (&Y)[CPL], doubl
         cs += Y[c] * cpR * kRu * iw;
       }
     }
-    hs = warp_sum(hs);
-    cs = warp_sum(cs);
+    hs = g.sum(hs);
+    cs = g.sum(cs);
     const double dT = (h - hs) / cs;
     T += dT;
     if (fabs(dT) <= 1e-12 * T) break;
@@ -527,8 +122,7 @@ struct InstParams {
   double* T;
   double* rhoYdot;     // MKS, component-major (may be null: T only)
   long long ncells;
-  int warp_bytes;
-  int Npad, Rpad, ldj, ldl;
+  GroupLayout L;
 };
 
 template <int CPL>
@@ -538,10 +132,16 @@ __global__ void __launch_bounds__(128) inst_rr_kernel(InstParams P) {
   if (threadIdx.x == 0) s_mech = P.mech;
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int N = P.mech.N, n = N + 1;
-  WarpBdf<CPL, double> B;
-  carve<CPL, double>(B, dsm + (size_t)w * P.warp_bytes, n, P.Npad, P.Rpad, P.ldj, P.ldl);
+  const int N = P.mech.N;
+  GrpScratch ms;
+  double* d = reinterpret_cast<double*>(dsm + (size_t)w * P.L.smem_bytes);
+  ms.C = d;
+  ms.gRT = d + P.L.Npad;
+  ms.hRT = d + 2 * P.L.Npad;
+  ms.q = d + 6 * P.L.Npad;
+  ms.r1 = ms.r2 = ms.r3 = ms.r4 = nullptr;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  const Grp<32> g(lane);
   for (long long c0 = (long long)blockIdx.x * (blockDim.x >> 5) + w; c0 < P.ncells; c0 += wstride) {
     double ry[CPL], Y[CPL];
     double rho = 0.0;
@@ -551,7 +151,7 @@ __global__ void __launch_bounds__(128) inst_rr_kernel(InstParams P) {
       ry[c] = (k < N) ? P.rhoY[(long long)k * P.ncells + c0] : 0.0;
       rho += ry[c];
     }
-    rho = warp_sum(rho);
+    rho = g.sum(rho);
     const double rinv = 1.0 / rho;
 #pragma unroll
     for (int c = 0; c < CPL; ++c) Y[c] = ry[c] * rinv;
@@ -559,18 +159,18 @@ __global__ void __launch_bounds__(128) inst_rr_kernel(InstParams P) {
     const double T = warp_t_from_hy<CPL>(s_mech, Y, h, P.T[c0], lane);
     if (lane == 0) P.T[c0] = T;
     if (P.rhoYdot) {
-      double y[CPL], F[CPL], yd[CPL];
+      Vec<CPL> y, F;
 #pragma unroll
       for (int c = 0; c < CPL; ++c) {
         const int k = lane + 32 * c;
-        y[c] = (k < N) ? ry[c] * 1.0e-3 : (k == N ? T : 0.0);  // kg/m^3 -> g/cm^3
-        F[c] = 0.0;
+        y.v[c] = (k < N) ? ry[c] * 1.0e-3 : (k == N ? T : 0.0);  // kg/m^3 -> g/cm^3
+        F.v[c] = 0.0;
       }
-      warp_rhs<CPL>(s_mech, B.ms, y, F, yd, lane);
+      const Vec<CPL> yd = grp_rhs<32, CPL>(&s_mech, ms, y, F, lane);
 #pragma unroll
       for (int c = 0; c < CPL; ++c) {
         const int k = lane + 32 * c;
-        if (k < N) P.rhoYdot[(long long)k * P.ncells + c0] = yd[c] * 1.0e3;  // g/cm^3/s -> kg/m^3/s
+        if (k < N) P.rhoYdot[(long long)k * P.ncells + c0] = yd.v[c] * 1.0e3;  // g/cm^3/s -> kg/m^3/s
       }
     }
     __syncwarp();
@@ -582,7 +182,7 @@ __global__ void __launch_bounds__(128) inst_rr_kernel(InstParams P) {
 // ------------------------------------------------------------------ handle
 struct b200chem_reactor {
   int device = 0;
-  int N = 0, R = 0, n = 0, cpl = 1;
+  int N = 0, R = 0, n = 0;
   b200chem_opts opts{};
   DevMech mech{};
   void* d_mech = nullptr;
@@ -595,31 +195,12 @@ struct b200chem_reactor {
   cudaEvent_t stage_ev = nullptr;
   bool stage_pending = false;
   int sm_count = 0;
-  int Npad = 32, Rpad = 32, ldj = 0, ldl = 0;
-  int warps_per_cta = 4;
-  void* d_tpc = nullptr;  // thread-per-cell scratch (Jacobians + LU factors)
-  size_t tpc_bytes = 0;
+  int smem_optin = 0;
+  void* d_work = nullptr;  // integrator scratch (group Jacobians, or thread-per-cell matrices)
+  size_t work_bytes = 0;
 };
 
 namespace {
-
-// warps per CTA (<= want) whose shared memory fits the opt-in per-block maximum
-int fit_warps(int warp_bytes, int want) {
-  int dev = 0, maxb = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxb, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  maxb -= 1024;  // static shared memory of the kernels
-  int w = want;
-  while (w > 1 && w * warp_bytes > maxb) --w;
-  return w;
-}
-
-int smem_warp_bytes(const b200chem_reactor* h, bool fp64_lu) {
-  size_t b = sizeof(double) * (5 * (size_t)h->Npad + 5 * (size_t)h->Rpad + (size_t)h->n * h->ldj);
-  b += (fp64_lu ? sizeof(double) : sizeof(float)) * (size_t)h->n * h->ldl;
-  b += sizeof(int) * (size_t)h->n;
-  return (int)((b + 15) & ~(size_t)15);
-}
 
 template <typename T>
 size_t push(std::vector<unsigned char>& buf, const std::vector<T>& v) {
@@ -629,75 +210,69 @@ size_t push(std::vector<unsigned char>& buf, const std::vector<T>& v) {
   return off;
 }
 
-template <int CPL, typename LUT>
-int set_kernel_smem(int bytes) {
-  CK(cudaFuncSetAttribute(react_kernel<CPL, LUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+int ensure_work(b200chem_reactor* h, size_t bytes, cudaStream_t st) {
+  if (bytes <= h->work_bytes) return 0;
+  if (h->d_work) {
+    CK(cudaStreamSynchronize(st));
+    cudaFree(h->d_work);
+    h->d_work = nullptr;
+    h->work_bytes = 0;
+  }
+  if (cudaMalloc(&h->d_work, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(B200CHEM_ENOMEM, "cannot allocate %zu bytes of integrator scratch", bytes);
+  }
+  h->work_bytes = bytes;
   return 0;
 }
 
-template <int CPL, typename LUT>
-int launch_react(b200chem_reactor* h, const ReactParams& P, int warps, cudaStream_t st) {
-  const int block = 32 * warps;
-  const int smem = P.warp_bytes * warps;
-  int err = set_kernel_smem<CPL, LUT>(smem);
+// Default lanes per cell of the group integrator for n = N+1 components.
+int default_group_lanes(int n) { return n <= 16 ? 8 : (n <= 32 ? 16 : 32); }
+
+int launch_group(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+  const int lut = h->opts.lu_fp64 ? 8 : 4;
+  const int G = h->opts.group_lanes > 0 ? h->opts.group_lanes : default_group_lanes(h->n);
+  if (G != 8 && G != 16 && G != 32) return set_err(B200CHEM_EINVAL, "group_lanes must be 8, 16 or 32");
+  const GroupVariant* v = nullptr;
+  for (int c = (h->n + G - 1) / G; c <= 8 && !v; ++c) v = find_group_variant(G, c, lut);  // next compiled CPL
+  if (!v) return set_err(B200CHEM_ETOOBIG, "no group variant for G=%d and n=%d", G, h->n);
+  GroupParams Q;
+  Q.L = group_layout(h->N, h->R, G, lut);
+  const int groups_per_cta = 128 / G;
+  const int smem = Q.L.smem_bytes * groups_per_cta;
+  if (smem > h->smem_optin - 2048)
+    return set_err(B200CHEM_ETOOBIG, "group integrator needs %d B of shared memory per CTA", smem);
+  int per_sm = v->occupancy(smem);
+  if (per_sm < 1) return set_err(B200CHEM_ETOOBIG, "group kernel does not fit on an SM");
+  if (h->opts.ctas_per_sm > 0) per_sm = std::min(per_sm, (int)h->opts.ctas_per_sm);
+  const long long need = (P.total + groups_per_cta - 1) / groups_per_cta;
+  const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)h->sm_count * per_sm));
+  int err = ensure_work(h, (size_t)(grid * groups_per_cta) * (size_t)Q.L.gbytes, st);
   if (err) return err;
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, react_kernel<CPL, LUT>, block, smem));
-  if (per_sm < 1) return set_err(B200CHEM_ETOOBIG, "react kernel does not fit on an SM (%d B smem)", smem);
-  long long need = (P.total + warps - 1) / warps;
-  long long grid = std::min<long long>(need, (long long)h->sm_count * per_sm);
-  if (grid < 1) grid = 1;
-  react_kernel<CPL, LUT><<<(unsigned)grid, block, smem, st>>>(P);
-  CK(cudaGetLastError());
+  Q.gscratch = static_cast<unsigned char*>(h->d_work);
+  CK(v->launch(P, Q, (int)grid, smem, st));
   return 0;
 }
 
-bool tpc_supported(int N) { return N == 9 || N == 21; }
-
-template <int NS, typename LUT>
-int launch_tpc(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
-  const int n = NS + 1;
-  const int smem = (int)(2 * sizeof(double) * NS * kTpcBlock);
-  CK(cudaFuncSetAttribute(react_tpc_kernel<NS, LUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, react_tpc_kernel<NS, LUT>, kTpcBlock, smem));
+int launch_thread_per_cell(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+  const int lut = h->opts.lu_fp64 ? 8 : 4;
+  int per_sm = 0, smem = 0;
+  CK(tpc_occupancy(h->N, lut, &per_sm, &smem));
   if (per_sm < 1) return set_err(B200CHEM_ETOOBIG, "thread-per-cell kernel does not fit on an SM");
   if (h->opts.ctas_per_sm > 0) per_sm = std::min(per_sm, (int)h->opts.ctas_per_sm);
-  long long need = (P.total + kTpcBlock - 1) / kTpcBlock;
-  long long grid = std::min<long long>(need, (long long)h->sm_count * per_sm);
-  if (grid < 1) grid = 1;
+  const long long need = (P.total + kTpcBlock - 1) / kTpcBlock;
+  const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)h->sm_count * per_sm));
   const long long nthr = grid * kTpcBlock;
-  const size_t bytes = (size_t)nthr * n * n * (sizeof(double) + sizeof(LUT));
-  if (bytes > h->tpc_bytes) {
-    if (h->d_tpc) {
-      CK(cudaStreamSynchronize(st));
-      cudaFree(h->d_tpc);
-      h->d_tpc = nullptr;
-      h->tpc_bytes = 0;
-    }
-    if (cudaMalloc(&h->d_tpc, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return set_err(B200CHEM_ENOMEM, "cannot allocate %zu bytes of integrator scratch", bytes);
-    }
-    h->tpc_bytes = bytes;
-  }
+  const int n = h->n;
+  int err = ensure_work(h, (size_t)nthr * n * n * (sizeof(double) + lut), st);
+  if (err) return err;
   TpcParams Q;
-  Q.J = static_cast<double*>(h->d_tpc);
-  Q.A = static_cast<void*>(static_cast<double*>(h->d_tpc) + (size_t)nthr * n * n);
+  Q.J = static_cast<double*>(h->d_work);
+  Q.A = static_cast<void*>(static_cast<double*>(h->d_work) + (size_t)nthr * n * n);
   Q.nthr = nthr;
   Q.setup_ratio = h->opts.setup_ratio > 0 ? h->opts.setup_ratio : 2;
-  react_tpc_kernel<NS, LUT><<<(unsigned)grid, kTpcBlock, smem, st>>>(P, Q);
-  CK(cudaGetLastError());
+  CK(tpc_launch(h->N, lut, P, Q, (int)grid, smem, st));
   return 0;
-}
-
-template <typename LUT>
-int launch_tpc_n(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
-  switch (h->N) {
-    case 9: return launch_tpc<9, LUT>(h, P, st);
-    case 21: return launch_tpc<21, LUT>(h, P, st);
-    default: return set_err(B200CHEM_EINVAL, "no thread-per-cell variant for N=%d", h->N);
-  }
 }
 
 int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long total, double dt, cudaStream_t st,
@@ -708,16 +283,21 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
     h->stage_pending = false;
     if (h->d_boxes) cudaFree(h->d_boxes);
     if (h->h_boxes) cudaFreeHost(h->h_boxes);
-    int cap = std::max(nbox, 64);
+    h->d_boxes = nullptr;
+    h->h_boxes = nullptr;
+    h->boxes_cap = 0;
+    const int cap = std::max(nbox, 64);
     CK(cudaMalloc(&h->d_boxes, sizeof(DevBox) * cap));
     CK(cudaMallocHost(&h->h_boxes, sizeof(DevBox) * cap));
     h->boxes_cap = cap;
   }
   if (h->stage_pending) CK(cudaEventSynchronize(h->stage_ev));
-  memcpy(h->h_boxes, boxes.data(), sizeof(DevBox) * nbox);
-  CK(cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(DevBox) * nbox, cudaMemcpyHostToDevice, st));
-  CK(cudaEventRecord(h->stage_ev, st));
-  h->stage_pending = true;
+  if (nbox > 0) {
+    memcpy(h->h_boxes, boxes.data(), sizeof(DevBox) * nbox);
+    CK(cudaMemcpyAsync(h->d_boxes, h->h_boxes, sizeof(DevBox) * nbox, cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(h->stage_ev, st));
+    h->stage_pending = true;
+  }
   CK(cudaMemsetAsync(h->d_scratch, 0, sizeof(unsigned long long) * (1 + kStCount), st));
   ReactParams P;
   P.mech = h->mech;
@@ -732,21 +312,10 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   P.queue = h->d_scratch;
   P.stats = reinterpret_cast<long long*>(h->d_scratch + 1);
   P.status = cell_status;
-  P.Npad = h->Npad;
-  P.Rpad = h->Rpad;
-  P.ldj = h->ldj;
-  P.ldl = h->ldl;
-  const bool fp64 = h->opts.lu_fp64 != 0;
-  P.warp_bytes = smem_warp_bytes(h, fp64);
-  const int warps = fit_warps(P.warp_bytes, h->opts.warps_per_cta > 0 ? h->opts.warps_per_cta : h->warps_per_cta);
-  int err;
-  const bool use_tpc = (h->opts.kernel == 1) || (h->opts.kernel == 0 && tpc_supported(h->N));
   if (h->opts.kernel == 1 && !tpc_supported(h->N))
     return set_err(B200CHEM_EINVAL, "thread-per-cell kernel requested but not compiled for N=%d", h->N);
   if (total > 0) {
-    if (use_tpc) err = fp64 ? launch_tpc_n<double>(h, P, st) : launch_tpc_n<float>(h, P, st);
-    else if (h->cpl == 1) err = fp64 ? launch_react<1, double>(h, P, warps, st) : launch_react<1, float>(h, P, warps, st);
-    else err = fp64 ? launch_react<2, double>(h, P, warps, st) : launch_react<2, float>(h, P, warps, st);
+    const int err = (h->opts.kernel == 1) ? launch_thread_per_cell(h, P, st) : launch_group(h, P, st);
     if (err) return err;
   }
   if (stats) {
@@ -780,6 +349,12 @@ DevArr to_dev(const b200chem_array4& a) {
   d.lo2 = a.lo[2];
   d.pad = 0;
   return d;
+}
+
+// shared memory of a 128-thread CTA of the evaluation kernels (one cell per warp)
+int eval_smem(const b200chem_reactor* h, GroupLayout* L) {
+  *L = group_layout(h->N, h->R, 32, 8);
+  return 4 * L->smem_bytes;
 }
 
 }  // namespace
@@ -816,12 +391,7 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
   h->N = N;
   h->R = R;
   h->n = N + 1;
-  h->cpl = (N + 1 <= 32) ? 1 : 2;
   h->opts = *o;
-  h->Npad = 32 * h->cpl;
-  h->Rpad = std::max(32, ((R + 31) / 32) * 32);
-  h->ldj = h->n | 1;
-  h->ldl = h->n | 1;
   // --- flatten to structure-of-arrays
   std::vector<double> mw(N), imw(N), nasa(15 * (size_t)N), arr(3 * (size_t)R), arrlo(3 * (size_t)R),
       arrrev(3 * (size_t)R), troe(4 * (size_t)R), sdnu(R), effm1;
@@ -905,6 +475,9 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
   cudaError_t e;
   if ((e = cudaGetDevice(&h->device)) != cudaSuccess) return fail(e, "cudaGetDevice");
   if ((e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device)) != cudaSuccess)
+    return fail(e, "cudaDeviceGetAttribute");
+  if ((e = cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device)) !=
+      cudaSuccess)
     return fail(e, "cudaDeviceGetAttribute");
   if ((e = cudaMalloc(&h->d_mech, buf.size())) != cudaSuccess) return fail(e, "cudaMalloc(mechanism)");
   if ((e = cudaMemcpy(h->d_mech, buf.data(), buf.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -1038,7 +611,7 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->d_scratch) cudaFree(h->d_scratch);
   if (h->d_boxes) cudaFree(h->d_boxes);
   if (h->h_boxes) cudaFreeHost(h->h_boxes);
-  if (h->d_tpc) cudaFree(h->d_tpc);
+  if (h->d_work) cudaFree(h->d_work);
   delete h;
   return 0;
 }
@@ -1047,27 +620,25 @@ static int eval_launch(b200chem_handle h, const double* y, const double* F, int6
                        int what) {
   if (!h || !y || !F || !out || ncells < 0) return set_err(B200CHEM_EINVAL, "bad arguments");
   if (ncells == 0) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   EvalParams P;
   P.mech = h->mech;
   P.y = y;
   P.F = F;
   P.out = out;
   P.ncells = ncells;
-  P.warp_bytes = smem_warp_bytes(h, true);
-  P.Npad = h->Npad;
-  P.Rpad = h->Rpad;
-  P.ldj = h->ldj;
-  P.ldl = h->ldl;
   P.what = what;
-  const int warps = fit_warps(P.warp_bytes, 4), smem = P.warp_bytes * warps;
-  const long long grid = std::min<long long>((ncells + warps - 1) / warps, (long long)h->sm_count * 16);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (h->cpl == 1) {
+  const int smem = eval_smem(h, &P.L);
+  const long long grid = std::min<long long>((ncells + 3) / 4, (long long)h->sm_count * 8);
+  int err = ensure_work(h, (size_t)(grid * 4) * (size_t)P.L.gbytes, st);
+  if (err) return err;
+  P.gscratch = static_cast<unsigned char*>(h->d_work);
+  if (h->n <= 32) {
     CK(cudaFuncSetAttribute(eval_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    eval_kernel<1><<<(unsigned)grid, 32 * warps, smem, st>>>(P);
+    eval_kernel<1><<<(unsigned)grid, 128, smem, st>>>(P);
   } else {
     CK(cudaFuncSetAttribute(eval_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    eval_kernel<2><<<(unsigned)grid, 32 * warps, smem, st>>>(P);
+    eval_kernel<2><<<(unsigned)grid, 128, smem, st>>>(P);
   }
   CK(cudaGetLastError());
   return 0;
@@ -1094,20 +665,15 @@ static int inst_launch(b200chem_handle h, const double* rhoY, const double* rhoH
   P.T = T;
   P.rhoYdot = rhoYdot;
   P.ncells = ncells;
-  P.warp_bytes = smem_warp_bytes(h, true);
-  P.Npad = h->Npad;
-  P.Rpad = h->Rpad;
-  P.ldj = h->ldj;
-  P.ldl = h->ldl;
-  const int warps = fit_warps(P.warp_bytes, 4), smem = P.warp_bytes * warps;
-  const long long grid = std::min<long long>((ncells + warps - 1) / warps, (long long)h->sm_count * 16);
+  const int smem = eval_smem(h, &P.L);
+  const long long grid = std::min<long long>((ncells + 3) / 4, (long long)h->sm_count * 16);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (h->cpl == 1) {
+  if (h->n <= 32) {
     CK(cudaFuncSetAttribute(inst_rr_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    inst_rr_kernel<1><<<(unsigned)grid, 32 * warps, smem, st>>>(P);
+    inst_rr_kernel<1><<<(unsigned)grid, 128, smem, st>>>(P);
   } else {
     CK(cudaFuncSetAttribute(inst_rr_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    inst_rr_kernel<2><<<(unsigned)grid, 32 * warps, smem, st>>>(P);
+    inst_rr_kernel<2><<<(unsigned)grid, 128, smem, st>>>(P);
   }
   CK(cudaGetLastError());
   return 0;
@@ -1125,3 +691,20 @@ int b200chem_t_from_hy(b200chem_handle h, const double* rhoY_mks, const double* 
 }
 
 }  // extern "C"
+
+namespace b200 {
+const GroupVariant* group_variants_g8(int* count);
+const GroupVariant* group_variants_g16(int* count);
+const GroupVariant* group_variants_g32(int* count);
+
+const GroupVariant* find_group_variant(int G, int CPL, int lut_bytes) {
+  int cnt = 0;
+  const GroupVariant* v = G == 8    ? group_variants_g8(&cnt)
+                          : G == 16 ? group_variants_g16(&cnt)
+                          : G == 32 ? group_variants_g32(&cnt)
+                                    : nullptr;
+  for (int i = 0; v && i < cnt; ++i)
+    if (v[i].CPL == CPL && v[i].lut_bytes == lut_bytes) return &v[i];
+  return nullptr;
+}
+}  // namespace b200

@@ -22,7 +22,7 @@
 //     is empty.
 // Every loop is bounded; failures end with a per-cell status code.
 #pragma once
-#include "bdf_warp.cuh"
+#include "bdf_group.cuh"
 
 namespace b200 {
 namespace tpc {

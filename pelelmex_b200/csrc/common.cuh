@@ -1,0 +1,110 @@
+// common.cuh -- data shared by the react kernels and the host code: box
+// views (amrex::Array4 mirrors), launch parameters, statistics slots, and the
+// per-group memory layout of the group integrator.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/b200chem.h"
+#include "bdf_group.cuh"
+
+namespace b200 {
+
+struct DevArr {
+  double* p;
+  long long js, ks, ns;
+  int lo0, lo1, lo2, pad;
+};
+struct DevIArr {
+  const int* p;
+  long long js, ks;
+  int lo0, lo1, lo2, pad;
+};
+struct DevBox {
+  int lo0, lo1, lo2, nx, ny, nz;
+  long long off;
+  DevArr rhoY, fY, T, rhoH, fH, fc;
+  DevIArr mask;
+};
+
+// stats slots in the scratch buffer (after the queue counter)
+enum { kStCells = 0, kStMasked, kStFailed, kStNst, kStNfe, kStNje, kStNlu, kStNetf, kStNcfn, kStMaxNfe,
+       kStMaxNst, kStCount };
+
+struct ReactParams {
+  DevMech mech;
+  const DevBox* boxes;
+  int nbox;
+  long long total;
+  double dt;
+  int max_steps;
+  int qmax;
+  double rtol;
+  const double* atol;
+  unsigned long long* queue;
+  long long* stats;
+  int* status;
+};
+
+__device__ __forceinline__ double* elem(const DevArr& a, int i, int j, int k) {
+  return a.p + (long long)(i - a.lo0) + (long long)(j - a.lo1) * a.js + (long long)(k - a.lo2) * a.ks;
+}
+
+
+// Per-group layout.  Shared: C, gRT, hRT, atol, Dsc, bvec [Npad] (double),
+// q [Rpad] (double), inverse [n][ldl] (LUT), fcol [Npad] (LUT), ipiv [n] (int).
+// Global: Jacobian [n][ldj] (column-major) and r1..r4 [Rpad] (double).
+struct GroupLayout {
+  int Npad, Rpad, n, ldj, ldl;
+  int smem_bytes;    // per group
+  long long gbytes;  // per group, global scratch
+};
+
+__host__ __device__ inline GroupLayout group_layout(int N, int R, int G, int lut_bytes) {
+  GroupLayout L;
+  L.n = N + 1;
+  L.Npad = ((L.n + G - 1) / G) * G;
+  L.Rpad = ((R + 31) / 32) * 32;
+  if (L.Rpad < 32) L.Rpad = 32;
+  L.ldj = L.n | 1;
+  L.ldl = L.n | 1;
+  long long b = 8LL * (6 * L.Npad + L.Rpad);
+  b += (long long)lut_bytes * ((long long)L.n * L.ldl + L.Npad);
+  b += 4LL * L.Npad;
+  L.smem_bytes = (int)((b + 15) & ~15LL);
+  L.gbytes = 8LL * ((long long)L.n * L.ldj + 4LL * L.Rpad);
+  L.gbytes = (L.gbytes + 255) & ~255LL;
+  return L;
+}
+
+struct GroupParams {
+  GroupLayout L;
+  unsigned char* gscratch;  // [groups in launch][L.gbytes]
+};
+
+// Host-side entry points of one compiled group-kernel variant.
+struct GroupVariant {
+  int G, CPL, lut_bytes;
+  // resident CTAs per SM for a block of 128 threads and `smem` bytes, or -1
+  int (*occupancy)(int smem);
+  cudaError_t (*launch)(const ReactParams& P, const GroupParams& Q, int grid, int smem, cudaStream_t st);
+};
+
+// Variants compiled in react_g*.cu; returns nullptr if (G, CPL, lut) has none.
+const GroupVariant* find_group_variant(int G, int CPL, int lut_bytes);
+
+struct TpcParams {
+  double* J;        // [n*n][threads] FP64 Jacobians, interleaved by thread
+  void* A;          // [n*n][threads] LU factors (float or double), interleaved
+  long long nthr;   // threads in the launch (interleave stride)
+  int setup_ratio;  // setup round when waiting * ratio >= needing an RHS
+};
+
+constexpr int kTpcBlock = 128;
+
+// Thread-per-cell kernels (react_tpc.cu): species counts with a variant.
+bool tpc_supported(int N);
+cudaError_t tpc_occupancy(int N, int lut_bytes, int* per_sm, int* smem);
+cudaError_t tpc_launch(int N, int lut_bytes, const ReactParams& P, const TpcParams& Q, int grid, int smem,
+                       cudaStream_t st);
+
+}  // namespace b200

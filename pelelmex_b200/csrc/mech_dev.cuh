@@ -4,16 +4,10 @@
 // This is the device side of what a CEPTR-generated mechanism provides to the
 // reference reactor (productionRate, aJacobian, species enthalpies/cp, reached
 // from PeleLMeX through eos.RTY2WDOT / T2Hi, Source/PeleLMeX_K.H:611,880-885).
-// Instead of straight-line generated code (which would serialise when lanes
-// take different reactions), the mechanism is table data in global memory in
-// structure-of-arrays form, read through the read-only path, and the work is
-// spread over the 32 lanes of a warp:
-//   * species-parallel: lane k owns species k (and lane N owns T) for thermo,
-//     concentrations and the production-rate gather;
-//   * reaction-parallel: lane j evaluates reactions j, j+32, ... (rates of
-//     progress, stored to per-warp shared memory);
-//   * column-parallel Jacobian: lane l owns column l and walks the reactions.
-// Everything here is FP64.
+// The mechanism is table data in global memory in structure-of-arrays form,
+// read through the read-only path; this file holds the tables and the
+// per-reaction rate evaluation shared by the group (group_mech.cuh) and the
+// thread-per-cell (bdf_thread.cuh) integrators.  Everything here is FP64.
 #pragma once
 #include <cstdint>
 
@@ -47,16 +41,11 @@ struct DevMech {
   const double* inc_nu;  // [nnz]
 };
 
-// Per-warp shared-memory scratch for the mechanism evaluation.
-struct MechSmem {
-  double* C;    // [Npad] concentrations (mol/cm^3)
-  double* gRT;  // [Npad] g/RT
-  double* hRT;  // [Npad] h/RT
-  double* r0;   // [Rpad] per-reaction scratch (q, or ceff)
-  double* r1;   // [Rpad] kf * mult
-  double* r2;   // [Rpad] kr * mult
-  double* r3;   // [Rpad] dq/dT
-  double* r4;   // [Rpad] q (Jacobian pass)
+// Species-indexed views used by the per-reaction evaluation (unit stride).
+struct SpView {
+  const double* C;    // concentrations (mol/cm^3)
+  const double* gRT;  // g/RT
+  const double* hRT;  // h/RT (Jacobian only)
 };
 
 // Per-lane components of one state vector, passed by value so that calls to
@@ -104,7 +93,7 @@ struct RxnEval {
 };
 
 template <bool JAC>
-__device__ __forceinline__ RxnEval eval_reaction(const DevMech& m, const MechSmem& s, int j, double T,
+__device__ __forceinline__ RxnEval eval_reaction(const DevMech& m, const SpView& s, int j, double T,
                                                  double lnT, double invT, double Ctot, double lnPRT) {
   const int R = m.R;
   RxnEval e;
@@ -198,276 +187,6 @@ __device__ __forceinline__ RxnEval eval_reaction(const DevMech& m, const MechSme
   e.dlnkf_dT = dlnkf;
   e.dkr_dT = dkr;
   return e;
-}
-
-// Thermo + concentrations for one cell. Lane k < N handles species k (and
-// k + 32 when CPL = 2).  Returns per-lane cp (mass, erg/g/K) and h (erg/g)
-// in the output arrays; writes C, gRT, hRT to shared memory.
-template <int CPL>
-__device__ __forceinline__ void species_state(const DevMech& m, const MechSmem& s, const double (&y)[CPL],
-                                              double T, double lnT, double (&cpk)[CPL], double (&hk)[CPL],
-                                              double (&dcpk)[CPL], int lane) {
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    const int k = lane + 32 * c;
-    cpk[c] = 0.0;
-    hk[c] = 0.0;
-    dcpk[c] = 0.0;
-    if (k < m.N) {
-      double cpR, hRT, sR, dcpR;
-      nasa7(m, k, T, lnT, cpR, hRT, sR, dcpR);
-      const double iw = __ldg(m.inv_mw + k);
-      s.C[k] = y[c] * iw;
-      s.gRT[k] = hRT - sR;
-      s.hRT[k] = hRT;
-      cpk[c] = cpR * kRu * iw;
-      hk[c] = hRT * kRu * T * iw;
-      dcpk[c] = dcpR * kRu * iw;
-    }
-  }
-}
-
-// Temperature (component N) broadcast from its owner lane.
-template <int CPL>
-__device__ __forceinline__ double get_T(const double (&y)[CPL], int N) {
-  const int owner = N & 31;
-  const int c = N >> 5;
-  double v = 0.0;
-#pragma unroll
-  for (int cc = 0; cc < CPL; ++cc)
-    if (cc == c) v = y[cc];
-  return __shfl_sync(kFull, v, owner);
-}
-
-// HP right-hand side of one cell (see the header of b200chem.h):
-//   ydot_k = W_k wdot_k + F_k,  ydot_T = (F_H - sum h_k ydot_k) / (sum y_k cp_k)
-template <int CPL>
-__device__ __noinline__ Vec<CPL> warp_rhs_v(const DevMech* mp, const MechSmem s, const Vec<CPL> yv, const Vec<CPL> Fv,
-                                           int lane) {
-  const DevMech& m = *mp;
-  const double(&y)[CPL] = yv.v;
-  const double(&F)[CPL] = Fv.v;
-  Vec<CPL> out;
-  double(&ydot)[CPL] = out.v;
-  const int N = m.N, R = m.R;
-  const double T = get_T<CPL>(y, N);
-  const double lnT = log(T), invT = 1.0 / T;
-  double cpk[CPL], hk[CPL], dcpk[CPL];
-  species_state<CPL>(m, s, y, T, lnT, cpk, hk, dcpk, lane);
-  double csum = 0.0;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-    if (lane + 32 * c < N) csum += y[c] * __ldg(m.inv_mw + lane + 32 * c);
-  const double Ctot = warp_sum(csum);
-  const double lnPRT = log(kPatm / (kRu * T));
-  __syncwarp();
-  for (int j = lane; j < R; j += 32) {
-    const RxnEval e = eval_reaction<false>(m, s, j, T, lnT, invT, Ctot, lnPRT);
-    double q = e.kf * e.pf - e.kr * e.pr;
-    if (__ldg(m.rtype + j) == 1) q *= e.M;
-    s.r0[j] = q;
-  }
-  __syncwarp();
-  double rcp = 0.0, hs = 0.0;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    const int k = lane + 32 * c;
-    if (k < N) {
-      double w = 0.0;
-      const int p0 = __ldg(m.inc_ptr + k), p1 = __ldg(m.inc_ptr + k + 1);
-      for (int p = p0; p < p1; ++p) w += __ldg(m.inc_nu + p) * s.r0[__ldg(m.inc_rxn + p)];
-      ydot[c] = w * __ldg(m.mw + k) + F[c];
-      rcp += y[c] * cpk[c];
-      hs += hk[c] * ydot[c];
-    }
-  }
-  rcp = warp_sum(rcp);
-  hs = warp_sum(hs);
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-    if (lane + 32 * c == N) ydot[c] = (F[c] - hs) / rcp;
-    else if (lane + 32 * c > N) ydot[c] = 0.0;
-  __syncwarp();
-  return out;
-}
-
-template <int CPL>
-__device__ __forceinline__ void warp_rhs(const DevMech& m, const MechSmem& s, const double (&y)[CPL],
-                                         const double (&F)[CPL], double (&ydot)[CPL], int lane) {
-  Vec<CPL> a, b;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    a.v[c] = y[c];
-    b.v[c] = F[c];
-  }
-  const Vec<CPL> r = warp_rhs_v<CPL>(&m, s, a, b, lane);
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) ydot[c] = r.v[c];
-}
-
-// Analytic Jacobian of the HP system into shared memory J[i*ldj + j]
-// (row i = equation, column j = variable), plus ydot (same as warp_rhs).
-template <int CPL>
-__device__ __noinline__ Vec<CPL> warp_jac_v(const DevMech* mp, const MechSmem s, const Vec<CPL> yv, const Vec<CPL> Fv,
-                                           double* J, int ldj, int lane) {
-  const DevMech& m = *mp;
-  const double(&y)[CPL] = yv.v;
-  const double(&F)[CPL] = Fv.v;
-  Vec<CPL> out;
-  double(&ydot)[CPL] = out.v;
-  const int N = m.N, R = m.R, n = N + 1;
-  const double T = get_T<CPL>(y, N);
-  const double lnT = log(T), invT = 1.0 / T;
-  double cpk[CPL], hk[CPL], dcpk[CPL];
-  species_state<CPL>(m, s, y, T, lnT, cpk, hk, dcpk, lane);
-  double csum = 0.0;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-    if (lane + 32 * c < N) csum += y[c] * __ldg(m.inv_mw + lane + 32 * c);
-  const double Ctot = warp_sum(csum);
-  const double lnPRT = log(kPatm / (kRu * T));
-  // zero J
-  for (int i = 0; i < n; ++i)
-#pragma unroll
-    for (int c = 0; c < CPL; ++c)
-      if (lane + 32 * c < n) J[i * ldj + lane + 32 * c] = 0.0;
-  __syncwarp();
-  // phase 1: per-reaction scalars (lane per reaction)
-  for (int j = lane; j < R; j += 32) {
-    const RxnEval e = eval_reaction<true>(m, s, j, T, lnT, invT, Ctot, lnPRT);
-    const int type = __ldg(m.rtype + j);
-    const double mult = (type == 1) ? e.M : 1.0;
-    double ceff = 0.0;
-    if (type == 1) ceff = e.kf * e.pf - e.kr * e.pr;
-    else if (type >= 2) ceff = e.dkf_dM * (e.pf - (e.kf > 0.0 ? e.kr / e.kf : 0.0) * e.pr);
-    s.r0[j] = ceff;
-    s.r1[j] = mult * e.kf;
-    s.r2[j] = mult * e.kr;
-    s.r3[j] = mult * (e.kf * e.dlnkf_dT * e.pf - e.dkr_dT * e.pr);
-    s.r4[j] = mult * (e.kf * e.pf - e.kr * e.pr);
-  }
-  __syncwarp();
-  // phase 2: column-parallel accumulation of d(wdot)/d(C_l) and d(wdot)/dT
-  for (int j = 0; j < R; ++j) {
-    const int type = __ldg(m.rtype + j);
-    const double ceff = s.r0[j], kfm = s.r1[j], krm = s.r2[j], dqdT = s.r3[j];
-    int spj[8], nuj[8];
-#pragma unroll
-    for (int sl = 0; sl < 8; ++sl) {
-      spj[sl] = __ldg(m.sp + sl * R + j);
-      nuj[sl] = __ldg(m.nu + sl * R + j);
-    }
-    const int e0 = (type != 0) ? __ldg(m.eff_ptr + j) : 0;
-    const int e1 = (type != 0) ? __ldg(m.eff_ptr + j + 1) : 0;
-#pragma unroll
-    for (int c = 0; c < CPL; ++c) {
-      const int l = lane + 32 * c;
-      double d = 0.0;
-      if (l < N) {
-        if (type != 0) {
-          double eff = 1.0;
-          for (int q = e0; q < e1; ++q)
-            if (__ldg(m.eff_sp + q) == l) eff += __ldg(m.eff_m1 + q);
-          d = eff * ceff;
-        }
-#pragma unroll
-        for (int sl = 0; sl < 4; ++sl) {
-          if (spj[sl] == l) {
-            const int v = -nuj[sl];
-            double p = v * ipow(s.C[l], v - 1);
-#pragma unroll
-            for (int s2 = 0; s2 < 4; ++s2)
-              if (s2 != sl && spj[s2] >= 0) p *= ipow(s.C[spj[s2]], -nuj[s2]);
-            d += kfm * p;
-          }
-          if (spj[sl + 4] == l) {
-            const int v = nuj[sl + 4];
-            double p = v * ipow(s.C[l], v - 1);
-#pragma unroll
-            for (int s2 = 0; s2 < 4; ++s2)
-              if (s2 != sl && spj[s2 + 4] >= 0) p *= ipow(s.C[spj[s2 + 4]], nuj[s2 + 4]);
-            d -= krm * p;
-          }
-        }
-      } else if (l == N) {
-        d = dqdT;
-      }
-      if (l <= N && d != 0.0) {
-#pragma unroll
-        for (int sl = 0; sl < 8; ++sl)
-          if (spj[sl] >= 0) J[spj[sl] * ldj + l] += (double)nuj[sl] * d;
-      }
-    }
-  }
-  __syncwarp();
-  // species rows: scale to mass units, compute ydot
-  double rcp = 0.0, hs = 0.0, drcp = 0.0, cpdot = 0.0;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    const int k = lane + 32 * c;
-    if (k < N) {
-      double w = 0.0;
-      const int p0 = __ldg(m.inc_ptr + k), p1 = __ldg(m.inc_ptr + k + 1);
-      for (int p = p0; p < p1; ++p) w += __ldg(m.inc_nu + p) * s.r4[__ldg(m.inc_rxn + p)];
-      ydot[c] = w * __ldg(m.mw + k) + F[c];
-      rcp += y[c] * cpk[c];
-      hs += hk[c] * ydot[c];
-      drcp += y[c] * dcpk[c];
-      cpdot += cpk[c] * ydot[c];
-    }
-  }
-  rcp = warp_sum(rcp);
-  hs = warp_sum(hs);
-  drcp = warp_sum(drcp);
-  cpdot = warp_sum(cpdot);
-  double Tdot = 0.0;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-    if (lane + 32 * c == N) Tdot = (F[c] - hs) / rcp;
-  Tdot = warp_sum(Tdot);
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    const int l = lane + 32 * c;
-    if (l == N) ydot[c] = Tdot;
-    else if (l > N) ydot[c] = 0.0;
-  }
-  // scale species rows: J[k][l] *= W_k / W_l (l < N), J[k][N] *= W_k  (lane = column l)
-  // and the T row: J[N][l] = -(sum_k h_k J[k][l] + (l<N ? Tdot cp_l : cpdot + Tdot drcp)) / rcp
-  // h_k and cp_l are needed by every lane: stash mass-specific h in gRT (no longer needed).
-#pragma unroll
-  for (int c = 0; c < CPL; ++c)
-    if (lane + 32 * c < N) s.gRT[lane + 32 * c] = hk[c];
-  __syncwarp();
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    const int l = lane + 32 * c;
-    if (l <= N) {
-      const double inv_wl = (l < N) ? __ldg(m.inv_mw + l) : 1.0;
-      double sum = 0.0;
-      for (int k = 0; k < N; ++k) {
-        const double v = J[k * ldj + l] * __ldg(m.mw + k) * inv_wl;
-        J[k * ldj + l] = v;
-        sum += s.gRT[k] * v;
-      }
-      J[N * ldj + l] = -(sum + ((l < N) ? Tdot * cpk[c] : cpdot + Tdot * drcp)) / rcp;
-    }
-  }
-  __syncwarp();
-  return out;
-}
-
-template <int CPL>
-__device__ __forceinline__ void warp_jac(const DevMech& m, const MechSmem& s, const double (&y)[CPL],
-                                         const double (&F)[CPL], double (&ydot)[CPL], double* J, int ldj, int lane) {
-  Vec<CPL> a, b;
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    a.v[c] = y[c];
-    b.v[c] = F[c];
-  }
-  const Vec<CPL> r = warp_jac_v<CPL>(&m, s, a, b, J, ldj, lane);
-#pragma unroll
-  for (int c = 0; c < CPL; ++c) ydot[c] = r.v[c];
 }
 
 }  // namespace b200

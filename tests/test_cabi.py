@@ -33,7 +33,7 @@ def test_struct_layouts_match_header():
     from pelelmex_b200 import _lib
     assert ctypes.sizeof(_lib.Array4) == 8 + 3 * 8 + 6 * 4
     assert ctypes.sizeof(_lib.BoxView) == 24 + 7 * ctypes.sizeof(_lib.Array4)
-    assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 9 * 4 + 4  # 9 int32 fields, padded to 8 bytes
+    assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 10 * 4  # two doubles and ten int32 fields
 
 
 def test_null_handle_is_rejected_without_gpu():

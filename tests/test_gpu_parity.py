@@ -38,9 +38,9 @@ def _dev(a, dtype=torch.float64):
 
 
 def run_gpu(name, f, rtol=1e-8, atol=1e-12, max_order=5, lu_fp64=False, typ=None, mask=None, max_steps=10000,
-            fY=None, fH=None, kernel="auto"):
+            fY=None, fH=None, kernel="auto", group_lanes=0):
     r = ReactorB200(name, rtol=rtol, atol=atol, max_order=max_order, lu_fp64=lu_fp64,
-                    max_steps=max_steps, kernel=kernel).init(2, f.ncells)
+                    max_steps=max_steps, kernel=kernel, group_lanes=group_lanes).init(2, f.ncells)
     if typ is not None:
         r.set_typ_vals_ode(typ)
     rhoY, T, rhoH = _dev(f.rhoY), _dev(f.T), _dev(f.rhoH)
@@ -114,7 +114,7 @@ def test_flame_ch4_sample(dt, orc_cache):
 
 
 def test_dodecane_two_components_per_lane(orc_cache):
-    """53 species: n = 54 > 32 exercises the two-components-per-lane path."""
+    """53 species: n = 54 components, several per lane."""
     mech = M.builtin("synth_c12_53")
     rng = np.random.default_rng(7)
     nm = mech.names
@@ -146,17 +146,28 @@ def test_dodecane_two_components_per_lane(orc_cache):
     assert eg.max() <= 3.0 * eo.max() + 1e-9
 
 
-@pytest.mark.parametrize("kernel", ["warp", "thread"])
+@pytest.mark.parametrize("kernel,lanes", [("thread", 0), ("group", 8), ("group", 16), ("group", 32)])
 @pytest.mark.parametrize("lu_fp64", [False, True])
-def test_both_kernels_and_lu_precisions(kernel, lu_fp64, orc_cache):
-    """Thread-per-cell and warp-per-cell kernels, FP32+refinement and FP64 LU."""
+def test_kernels_group_sizes_and_lu_precisions(kernel, lanes, lu_fp64, orc_cache):
+    """Thread-per-cell and group integrators (8/16/32 lanes per cell), FP32
+    inverse + FP64 refinement and FP64 inverse."""
     mech = M.builtin("synth_ch4_21")
     f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 1024, seed=13), dt=1e-5)
-    g = run_gpu("synth_ch4_21", f, kernel=kernel, lu_fp64=lu_fp64)
+    g = run_gpu("synth_ch4_21", f, kernel=kernel, lu_fp64=lu_fp64, group_lanes=lanes)
     o = orc_cache("synth_ch4_21").react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12,
                                         max_order=5)
     assert (g["status"] == 0).all()
-    compare(f, g, o, f"{kernel} kernel, lu_fp64={lu_fp64}")
+    compare(f, g, o, f"{kernel} kernel G={lanes}, lu_fp64={lu_fp64}")
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_group_sizes_on_h2(lanes, orc_cache):
+    """Group sizes on the 10-component system (1 or 2 components per lane)."""
+    f = W.premixed_h2(M.builtin("synth_h2_9"), edge=8)
+    g = run_gpu("synth_h2_9", f, group_lanes=lanes)
+    o = orc_cache("synth_h2_9").react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12,
+                                      max_order=5)
+    compare(f, g, o, f"synth_h2_9 G={lanes}")
 
 
 def test_fp64_lu_variant(orc_cache):
