@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Chemistry-step throughput of the B200 HP reactor (cells/s per chem step).
+
+Workload: the drm19-shaped flame field (21 species + T, 84 reactions of the
+bundled synthetic CH4/air mechanism; the drm19 mechanism file itself is not
+available), 128^3 = 2,097,152 cells, dt_react = 1e-6 s, P = 1 atm, rtol 1e-8 /
+atol 1e-12, max order 5 (the parity settings of the dense-direct BDF).  One
+step = one react call over the whole field, state restored between steps
+(inputs of 750 MB, far larger than L2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank reacts its own copy of
+the field (cells shard with no exchange), so scaling is weak and the value is
+the cells of all ranks over the slowest rank's device time.
+
+`--impl reference` times the CPU restatement of the dense-direct BDF (the
+oracle; the reference's own CVODE reactor cannot be built here) on the host
+cores, rank 0 only, over a seeded random sample of the same field.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cells/s per chem step (drm19 128^3) at ≤1e-4 T err: hybrid vs plain GPU BDF"
+UNIT = "cells/s"
+MECH = "synth_ch4_21"
+RTOL, ATOL, QMAX, MAXSTEPS = 1e-8, 1e-12, 5, 10000
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--edge", type=int, default=128)
+    p.add_argument("--dt", type=float, default=1e-6)
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(args):
+    return {"workload": f"flame_ch4 {args.edge}^3 drm19-shaped (synth_ch4_21: 21 species + T, 84 reactions), "
+                        f"dt_react {args.dt:g} s, P 1 atm",
+            "mechanism": MECH, "cells": args.edge ** 3, "dt_react": args.dt, "rtol": RTOL, "atol": ATOL,
+            "max_order": QMAX, "integrator": "plain GPU BDF (FP64 state/rates, FP32 Newton inverse + FP64 refinement)",
+            "l2": "inputs 750 MB > L2, state restored from a device copy between steps"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms (read only)."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = bus_id
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.bus_id:
+            cmd += ["-i", self.bus_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------------------- utilities
+def load_field(args):
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    mech = mechmod.builtin(MECH)
+    return mech, workloads.flame_ch4(mech, edge=args.edge, dt=args.dt)
+
+
+def fp64_peak_tflops(torch, dev):
+    """Live FP64 reference peak: cuBLAS DGEMM 8192^3, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def sample_field(mech, args, n, seed):
+    """n seeded random cells of the full field, generated directly."""
+    from pelelmex_b200 import workloads
+    idx = workloads.sample_cells(args.edge ** 3, n, seed=seed)
+    return workloads.flame_ch4(mech, edge=args.edge, dt=args.dt, cells=idx)
+
+
+def cpu_sample_run(mech, args, seconds: float, nthreads: int = 0):
+    """Time the oracle on a seeded random sample sized to about `seconds`.
+    Returns (cells/s, sample cells, threads, seconds taken)."""
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod
+    o = orc.Oracle(mechmod.flatten(mech))
+    threads = nthreads or orc.max_threads()
+    total = args.edge ** 3
+    n = min(total, max(256, 64 * threads))
+    while True:
+        sub = sample_field(mech, args, n, 777)
+        t0 = time.perf_counter()
+        o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=RTOL, atol=ATOL,
+                max_order=QMAX, max_steps=MAXSTEPS, nthreads=threads)
+        el = time.perf_counter() - t0
+        if el >= 0.3 * seconds or n >= total:
+            return n / el, n, threads, el
+        n = min(total, int(n * min(8.0, max(1.5, 0.6 * seconds / max(el, 1e-3)))))
+
+
+def emit(line):
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    cfg = workload_config(args)
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod
+    mech = mechmod.builtin(MECH)
+    total = args.edge ** 3
+    o = orc.Oracle(mechmod.flatten(mech))
+    threads = orc.max_threads()
+    per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    rate, n, _, _ = cpu_sample_run(mech, args, per_step, threads)
+    times = []
+    for s in range(args.warmup + args.steps):
+        sub = sample_field(mech, args, n, 1000 + s)
+        t0 = time.perf_counter()
+        o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=RTOL, atol=ATOL, max_order=QMAX,
+                max_steps=MAXSTEPS, nthreads=threads)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = n * len(times) / sum(times)
+    ms_full = total / value * 1e3
+    sample = (f"{n} seeded random cells of the {args.edge}^3 field per step, CPU restatement of the dense-direct "
+              f"BDF (OpenMP, {threads} threads), extrapolated linearly to {total} cells")
+    emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_full, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+          "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+
+
+# ------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from pelelmex_b200 import perfmodel
+    from pelelmex_b200.reactor import ReactorB200
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    props = torch.cuda.get_device_properties(dev)
+    bus = getattr(props, "pci_bus_id", None)
+    bus_id = f"{props.pci_domain_id:08x}:{bus:02x}:{props.pci_device_id:02x}.0" if bus is not None else None
+    mech, field = load_field(args)
+    nc = field.ncells
+    N = mech.n_species
+    cfg = workload_config(args)
+
+    r = ReactorB200(MECH, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    base = {k: torch.tensor(getattr(field, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
+    rY, T, rH = (torch.empty_like(base[k]) for k in ("rhoY", "T", "rhoH"))
+    fct = torch.zeros(nc, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def restore():
+        rY.copy_(base["rhoY"])
+        T.copy_(base["T"])
+        rH.copy_(base["rhoH"])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up; the first call also collects the integrator's counters
+    counters = None
+    for w in range(args.warmup):
+        restore()
+        res = r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt, stats=(w == 0))
+        if w == 0:
+            counters = res[2]
+    torch.cuda.synchronize()
+
+    # timed region: K steps, each bracketed by events on the launching stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(bus_id) as clk:
+        for s in range(args.steps):
+            restore()
+            ev[s][0].record(stream)
+            r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
+            ev[s][1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nc / (ms * 1e-3)
+
+    # end to end through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.from_numpy(np.ascontiguousarray(getattr(field, k))).pin_memory()
+                for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
+        out = {k: torch.empty_like(host[k]).pin_memory() for k in ("rhoY", "T", "rhoH")}
+        fct_h = torch.empty(nc, dtype=torch.float64).pin_memory()
+        dbuf = {k: torch.empty_like(base[k]) for k in host}
+        h2d = sum(t.numel() * t.element_size() for t in host.values())
+        d2h = sum(t.numel() * t.element_size() for t in out.values()) + fct_h.numel() * 8
+
+        def e2e_step():
+            for k in host:
+                dbuf[k].copy_(host[k], non_blocking=True)
+            r.react_flat(dbuf["rhoY"], dbuf["frhoY"], dbuf["T"], dbuf["rhoH"], dbuf["frhoH"], fct,
+                         dt_react=field.dt)
+            for k in out:
+                out[k].copy_(dbuf[k], non_blocking=True)
+            fct_h.copy_(fct, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * nc / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+
+    # roofline of the react kernel (FP64 algorithmic flops per launch)
+    counts = perfmodel.op_counts(r.flat)
+    cn = {k: counters[k] / nc for k in ("nfe", "nje", "nlu", "nst")}
+    fl_cell = perfmodel.flops_per_cell(counts, cn["nfe"], cn["nje"], cn["nlu"], cn["nfe"], cn["nst"])
+    achieved = fl_cell * nc / (ms * 1e-3) / 1e12
+    peak = fp64_peak_tflops(torch, dev)
+    traffic = None
+    tj = ROOT / "profiles" / "traffic.json"
+    if tj.exists():
+        try:
+            tr = json.loads(tj.read_text())
+            if tr.get("edge") == args.edge and tr.get("dt") == args.dt:
+                traffic = tr.get("bytes_per_launch")
+        except (ValueError, OSError):
+            traffic = None
+    roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": "react_group_kernel",
+            "peak_source": "measured live: cuBLAS DGEMM 8192^3 best of 5 (FP64 has no entry in the measured-peaks "
+                           "file)",
+            "flops_per_cell": fl_cell, "per_cell_counters": cn,
+            "hbm_algorithmic_bytes_per_launch": perfmodel.bytes_per_cell(N) * nc}
+
+    cpu = None
+    if world == 1 and rank == 0:
+        rate, n, threads, el = cpu_sample_run(mech, args, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} seeded random cells of the {args.edge}^3 field, oracle restatement of the dense-direct "
+                         f"BDF on {threads} host threads ({el:.1f} s), extrapolated to cells/s"}
+
+    if rank == 0:
+        emit({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+              "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded flame-like field; synthetic "
+              "drm19-shaped mechanism)", "config": cfg, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+              "gpu_launches": args.steps, "clocks": clk.summary(), "step_ms": step_ms,
+              "counters": {k: int(v) for k, v in counters.items()}})
+    r.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
