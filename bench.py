@@ -51,13 +51,17 @@ def parse():
     p.add_argument("--dt", type=float, default=1e-6)
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--cells", type=int, default=0,
+                   help="react only this many seeded random cells of the field (small profiling cases)")
     return p.parse_args()
 
 
 def workload_config(args):
-    return {"workload": f"flame_ch4 {args.edge}^3 drm19-shaped (synth_ch4_21: 21 species + T, 84 reactions), "
+    sub = f" ({args.cells} seeded random cells)" if args.cells else ""
+    return {"workload": f"flame_ch4 {args.edge}^3{sub} drm19-shaped (synth_ch4_21: 21 species + T, 84 reactions), "
                         f"dt_react {args.dt:g} s, P 1 atm",
-            "mechanism": MECH, "cells": args.edge ** 3, "dt_react": args.dt, "rtol": RTOL, "atol": ATOL,
+            "mechanism": MECH, "cells": args.cells or args.edge ** 3, "dt_react": args.dt, "rtol": RTOL, "atol": ATOL,
             "max_order": QMAX, "integrator": "plain GPU BDF (FP64 state/rates, FP32 Newton inverse + FP64 refinement)",
             "l2": "inputs 750 MB > L2, state restored from a device copy between steps"}
 
@@ -126,6 +130,8 @@ class ClockSampler:
 def load_field(args):
     from pelelmex_b200 import mechanism as mechmod, workloads
     mech = mechmod.builtin(MECH)
+    if args.cells:
+        return mech, sample_field(mech, args, args.cells, 4242)
     return mech, workloads.flame_ch4(mech, edge=args.edge, dt=args.dt)
 
 
@@ -332,7 +338,7 @@ def run_b200(args, rank, world, local_rank):
             "hbm_algorithmic_bytes_per_launch": perfmodel.bytes_per_cell(N) * nc}
 
     cpu = None
-    if world == 1 and rank == 0:
+    if world == 1 and rank == 0 and not args.no_cpu:
         rate, n, threads, el = cpu_sample_run(mech, args, args.cpu_seconds)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{n} seeded random cells of the {args.edge}^3 field, oracle restatement of the dense-direct "
