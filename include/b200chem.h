@@ -172,6 +172,22 @@ int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY
                         const int32_t* mask, int64_t ncells, double* dt_react, double* time,
                         void* stream, int32_t* cell_status, b200chem_stats* stats);
 
+/* Allocation-free form of b200chem_react_flat (same arguments, same results).
+ * No reference counterpart: PelePhysics has no allocation-free react.  It
+ * calls no cudaMalloc/cudaFree or other allocating routine: its scratch is a
+ * fixed 24 MiB device array of the library, whose address is looked up once
+ * per device (cudaGetSymbolAddress) on the first call on that device -- make
+ * that first call before any stream capture.  It runs the group integrator
+ * (opts.kernel 0 or 2) with the grid capped to fit the fixed scratch, and
+ * returns B200CHEM_ETOOBIG when one CTA per SM of the mechanism's integrator
+ * scratch does not fit.  The scratch is shared by all handles on a device:
+ * calls that overlap in time (other streams, other host threads) race on it
+ * and must be serialised by the caller. */
+int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T,
+                                double* rhoH, const double* extF_rhoH, double* fctCount,
+                                const int32_t* mask, int64_t ncells, double* dt_react, double* time,
+                                void* stream, int32_t* cell_status, b200chem_stats* stats);
+
 /* ReactorBase::close (Source/PeleLMeX.cpp:26). */
 int b200chem_destroy(b200chem_handle h);
 

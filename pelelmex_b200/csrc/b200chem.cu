@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -600,6 +601,152 @@ int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY
   const int err = do_react(h, boxes, ncells, *dt_react, static_cast<cudaStream_t>(stream), cell_status, stats);
   if (time) *time += *dt_react;
   return err;
+}
+
+// ------------------------------------------------ allocation-free react
+// Fixed device scratch of b200chem_react_flat_noalloc: [0, 256) the work
+// queue counter and the statistics slots (must start at zero, cleared by each
+// call), [256, 1024) the one box descriptor of the flat call, then the group
+// integrator's per-group global scratch (Jacobian and per-reaction
+// coefficients, written before they are read).
+constexpr size_t kNoAllocScratchBytes = 24u << 20;  // 24 MiB
+constexpr size_t kNoAllocBoxOffset = 256;
+constexpr size_t kNoAllocWorkOffset = 1024;
+static_assert(sizeof(unsigned long long) * (1 + kStCount) <= kNoAllocBoxOffset, "counters overflow their slot");
+static_assert(sizeof(DevBox) <= kNoAllocWorkOffset - kNoAllocBoxOffset, "box descriptor overflows its slot");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device (cudaGetSymbolAddress; no allocation).
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return set_err(B200CHEM_EINVAL, "device %d out of range", device);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T,
+                                           double* rhoH, const double* extF_rhoH, double* fctCount,
+                                           const int32_t* mask, int64_t ncells, double* dt_react, double* time,
+                                           void* stream, int32_t* cell_status, b200chem_stats* stats) {
+  if (!h || ncells < 0 || !dt_react) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (ncells > 0 && (!rhoY || !extF_rhoY || !T || !rhoH || !extF_rhoH))
+    return set_err(B200CHEM_EINVAL, "null state array");
+  if (!(*dt_react > 0.0)) return set_err(B200CHEM_EINVAL, "dt_react must be positive");
+  if (ncells > 0x7fffffffLL) return set_err(B200CHEM_ETOOBIG, "ncells above 2^31-1 in one flat call");
+  if (h->opts.kernel == 1)
+    return set_err(B200CHEM_EINVAL, "the allocation-free react runs the group integrator only (kernel 0 or 2)");
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  if (dev != h->device) return set_err(B200CHEM_EINVAL, "current device %d is not the reactor's device %d", dev,
+                                       h->device);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // integrator variant and launch shape (the group kernel of react_flat)
+  const int lut = h->opts.lu_fp64 ? 8 : 4;
+  const int G = h->opts.group_lanes > 0 ? h->opts.group_lanes : default_group_lanes(h->n);
+  if (G != 8 && G != 16 && G != 32) return set_err(B200CHEM_EINVAL, "group_lanes must be 8, 16 or 32");
+  const GroupVariant* v = nullptr;
+  for (int c = (h->n + G - 1) / G; c <= 8 && !v; ++c) v = find_group_variant(G, c, lut);
+  if (!v) return set_err(B200CHEM_ETOOBIG, "no group variant for G=%d and n=%d", G, h->n);
+  GroupParams Q;
+  Q.L = group_layout(h->N, h->R, G, lut);
+  const int groups_per_cta = 128 / G;
+  const int smem = Q.L.smem_bytes * groups_per_cta;
+  if (smem > h->smem_optin - 2048)
+    return set_err(B200CHEM_ETOOBIG, "group integrator needs %d B of shared memory per CTA", smem);
+  int per_sm = v->occupancy(smem);
+  if (per_sm < 1) return set_err(B200CHEM_ETOOBIG, "group kernel does not fit on an SM");
+  if (h->opts.ctas_per_sm > 0) per_sm = std::min(per_sm, (int)h->opts.ctas_per_sm);
+  // the grid is capped by the fixed scratch: at least one CTA per SM must fit
+  const long long cta_bytes = (long long)groups_per_cta * Q.L.gbytes;
+  const long long cap_ctas = (long long)(kNoAllocScratchBytes - kNoAllocWorkOffset) / cta_bytes;
+  if (cap_ctas < h->sm_count)
+    return set_err(B200CHEM_ETOOBIG,
+                   "allocation-free react needs %lld B of scratch for one CTA per SM (%d SMs x %lld B); the fixed "
+                   "scratch holds %zu B",
+                   cta_bytes * h->sm_count, h->sm_count, cta_bytes, kNoAllocScratchBytes - kNoAllocWorkOffset);
+  const long long rows = std::min<long long>(per_sm, cap_ctas / h->sm_count);
+  const long long need = (ncells + groups_per_cta - 1) / groups_per_cta;
+  const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)h->sm_count * rows));
+  unsigned char* base = nullptr;
+  int err = noalloc_scratch(dev, &base);
+  if (err) return err;
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(base);
+  DevBox* d_box = reinterpret_cast<DevBox*>(base + kNoAllocBoxOffset);
+  // queue counter and statistics start at zero
+  CK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * (1 + kStCount), st));
+  if (ncells > 0) {
+    DevBox d{};
+    d.nx = (int)ncells;
+    d.ny = d.nz = 1;
+    d.off = 0;
+    auto mk = [&](const double* p) {
+      DevArr a{};
+      a.p = const_cast<double*>(p);
+      a.js = a.ks = ncells;
+      a.ns = ncells;
+      return a;
+    };
+    d.rhoY = mk(rhoY);
+    d.fY = mk(extF_rhoY);
+    d.T = mk(T);
+    d.rhoH = mk(rhoH);
+    d.fH = mk(extF_rhoH);
+    d.fc = mk(fctCount);
+    d.mask.p = mask;
+    d.mask.js = d.mask.ks = ncells;
+    // pageable source: the copy is staged before cudaMemcpyAsync returns
+    CK(cudaMemcpyAsync(d_box, &d, sizeof(DevBox), cudaMemcpyHostToDevice, st));
+    ReactParams P;
+    P.mech = h->mech;
+    P.boxes = d_box;
+    P.nbox = 1;
+    P.total = ncells;
+    P.dt = *dt_react;
+    P.max_steps = h->opts.max_steps;
+    P.qmax = h->opts.max_order;
+    P.rtol = h->opts.rtol;
+    P.atol = h->d_atol;
+    P.queue = counters;
+    P.stats = reinterpret_cast<long long*>(counters + 1);
+    P.status = cell_status;
+    Q.gscratch = base + kNoAllocWorkOffset;
+    CK(v->launch(P, Q, (int)grid, smem, st));
+  }
+  if (stats) {
+    long long st_h[kStCount];
+    CK(cudaMemcpyAsync(st_h, counters + 1, sizeof(st_h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    stats->n_cells = st_h[kStCells];
+    stats->n_masked = st_h[kStMasked];
+    stats->n_failed = st_h[kStFailed];
+    stats->nst = st_h[kStNst];
+    stats->nfe = st_h[kStNfe];
+    stats->nje = st_h[kStNje];
+    stats->nlu = st_h[kStNlu];
+    stats->netf = st_h[kStNetf];
+    stats->ncfn = st_h[kStNcfn];
+    stats->max_nfe = (int32_t)st_h[kStMaxNfe];
+    stats->max_nst = (int32_t)st_h[kStMaxNst];
+    if (time) *time += *dt_react;
+    if (stats->n_failed > 0) return set_err(B200CHEM_EINTEGRATE, "%lld cell(s) failed to integrate", stats->n_failed);
+    return 0;
+  }
+  if (time) *time += *dt_react;
+  return 0;
 }
 
 int b200chem_destroy(b200chem_handle h) {
