@@ -94,7 +94,9 @@ typedef struct b200chem_opts {
   int32_t verbose;
   int32_t kernel;        /* 0: auto (group integrator); 1: thread-per-cell (only
                             species counts with a compiled variant); 2: group
-                            integrator                                           */
+                            integrator; 3: round-based integrator (rhs / ctrl /
+                            setup kernels over compacted cell lists; species
+                            counts with a compiled variant)                    */
   int32_t setup_ratio;   /* thread-per-cell: a warp runs a Jacobian/LU round when
                             (cells waiting) * setup_ratio >= (cells needing an
                             RHS); 0 = default (2)                                */

@@ -199,6 +199,15 @@ struct b200chem_reactor {
   int smem_optin = 0;
   void* d_work = nullptr;  // integrator scratch (group Jacobians, or thread-per-cell matrices)
   size_t work_bytes = 0;
+  // round-based integrator
+  void* d_rounds = nullptr;  // cell state of one chunk + its three slot lists
+  size_t rounds_bytes = 0;
+  void* d_rwarp = nullptr;   // per-warp scratch of the setup kernel
+  size_t rwarp_bytes = 0;
+  int* d_rcnt = nullptr;     // list counters [A, B, S]
+  int* h_rcnt = nullptr;     // pinned copy of one counter
+  RoundsGrids rgrid{};
+  int rgrid_lut = 0;
 };
 
 namespace {
@@ -276,6 +285,127 @@ int launch_thread_per_cell(b200chem_reactor* h, const ReactParams& P, cudaStream
   return 0;
 }
 
+// Cell-state budget of one chunk of the round-based integrator.
+constexpr long long kRoundsBudgetBytes = 24LL << 30;
+// Rounds between checks of the live-cell count (one host sync each).
+constexpr int kRoundsCheckEvery = 4;
+
+int ensure_buffer(void** p, size_t* have, size_t bytes, cudaStream_t st, const char* what) {
+  if (bytes <= *have) return 0;
+  if (*p) {
+    CK(cudaStreamSynchronize(st));
+    cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+  }
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_err(B200CHEM_ENOMEM, "cannot allocate %zu bytes of %s", bytes, what);
+  }
+  *have = bytes;
+  return 0;
+}
+
+// Round-based integrator: rhs / ctrl / setup kernels over compacted lists,
+// chunk by chunk (see react_rounds.cu).
+int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+  if (!rounds_supported(h->N))
+    return set_err(B200CHEM_EINVAL, "round-based integrator not compiled for N=%d", h->N);
+  const int lut = h->opts.lu_fp64 ? 8 : 4;
+  const RoundsSetupLayout SL = rounds_setup_layout(h->N, h->R, lut);
+  if (4 * SL.smem_per_warp > h->smem_optin - 2048)
+    return set_err(B200CHEM_ETOOBIG, "setup kernel needs %d B of shared memory per CTA", 4 * SL.smem_per_warp);
+  if (h->rgrid_lut != lut) {
+    CK(rounds_grids_for(h->N, lut, SL, h->sm_count, &h->rgrid));
+    h->rgrid_lut = lut;
+  }
+  // chunk capacity from the state budget (and the free device memory)
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  const long long per_cell = rounds_state_bytes_per_cell(h->N, lut);
+  long long budget = std::min<long long>(kRoundsBudgetBytes, (long long)((free_b + h->rounds_bytes) * 0.6));
+  long long cap = std::min<long long>(P.total, std::max<long long>(1024, budget / per_cell));
+  cap = std::min<long long>(cap, 1LL << 30);
+  const size_t state_bytes = (size_t)per_cell * cap + 16 * 256;
+  int err = ensure_buffer(&h->d_rounds, &h->rounds_bytes, state_bytes, st, "round-integrator state");
+  if (err) return err;
+  err = ensure_buffer(&h->d_rwarp, &h->rwarp_bytes, (size_t)h->rgrid.setup * 4 * SL.gbytes_per_warp, st,
+                      "setup scratch");
+  if (err) return err;
+  if (!h->d_rcnt) {
+    CK(cudaMalloc(&h->d_rcnt, 4 * sizeof(int)));
+    CK(cudaMallocHost(&h->h_rcnt, sizeof(int)));
+  }
+  RoundsParams R;
+  R.P = P;
+  R.SL = SL;
+  R.S = rounds_carve(h->d_rounds, cap, h->N, lut);
+  // the three slot lists follow the carved arrays (each rounded to 256 B)
+  int* lists = nullptr;
+  {
+    const long long n = h->N + 1;
+    size_t used = 0;
+    auto rnd = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    used += rnd(8ull * (rounds::kRCellD) * cap);
+    used += rnd(8ull * (kZn + 7) * n * cap);
+    used += rnd(4ull * rounds::kRCellI * cap);
+    used += rnd(8ull * n * n * cap);
+    used += rnd((size_t)lut * n * n * cap);
+    lists = reinterpret_cast<int*>(static_cast<unsigned char*>(h->d_rounds) + used);
+    if (used + 12ull * cap > h->rounds_bytes)
+      return set_err(B200CHEM_ECUDA, "round-integrator state layout overflows its buffer");
+  }
+  int* listA = lists;
+  int* listB = lists + cap;
+  int* listS = lists + 2 * cap;
+  int* cntA = h->d_rcnt;
+  int* cntB = h->d_rcnt + 1;
+  int* cntS = h->d_rcnt + 2;
+  R.wscratch = static_cast<unsigned char*>(h->d_rwarp);
+  const long long max_rounds = 64LL * std::max(1, (int)h->opts.max_steps) + 1024;
+  for (long long chunk0 = 0; chunk0 < P.total; chunk0 += cap) {
+    R.chunk0 = chunk0;
+    R.nchunk = std::min<long long>(cap, P.total - chunk0);
+    CK(cudaMemsetAsync(h->d_rcnt, 0, 4 * sizeof(int), st));
+    R.list_in = nullptr;
+    R.cnt_in = nullptr;
+    R.list_out = listA;
+    R.cnt_out = cntA;
+    R.list_setup = listS;
+    R.cnt_setup = cntS;
+    CK(rounds_launch(h->N, lut, kRoundsStart, R, h->rgrid, 0, st));
+    int* lst[2] = {listA, listB};
+    int* cnt[2] = {cntA, cntB};
+    int cur = 0;
+    for (long long round = 0;; ++round) {
+      if (round >= max_rounds) return set_err(B200CHEM_EINTEGRATE, "round-based integrator did not finish");
+      R.list_in = lst[cur];
+      R.cnt_in = cnt[cur];
+      R.list_out = lst[1 - cur];
+      R.cnt_out = cnt[1 - cur];
+      R.list_setup = listS;
+      R.cnt_setup = cntS;
+      CK(rounds_launch(h->N, lut, kRoundsRhs, R, h->rgrid, 0, st));
+      CK(cudaMemsetAsync(cnt[1 - cur], 0, sizeof(int), st));
+      CK(cudaMemsetAsync(cntS, 0, sizeof(int), st));
+      CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 1, st));
+      R.list_in = listS;
+      R.cnt_in = cntS;
+      CK(rounds_launch(h->N, lut, kRoundsSetup, R, h->rgrid, 0, st));
+      // cells coming back from a setup always ask for a right-hand side next
+      CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 0, st));
+      cur = 1 - cur;
+      if ((round + 1) % kRoundsCheckEvery == 0) {
+        CK(cudaMemcpyAsync(h->h_rcnt, cnt[cur], sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (*h->h_rcnt == 0) break;
+      }
+    }
+  }
+  return 0;
+}
+
 int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long total, double dt, cudaStream_t st,
              int32_t* cell_status, b200chem_stats* stats) {
   const int nbox = (int)boxes.size();
@@ -316,7 +446,9 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   if (h->opts.kernel == 1 && !tpc_supported(h->N))
     return set_err(B200CHEM_EINVAL, "thread-per-cell kernel requested but not compiled for N=%d", h->N);
   if (total > 0) {
-    const int err = (h->opts.kernel == 1) ? launch_thread_per_cell(h, P, st) : launch_group(h, P, st);
+    const int err = (h->opts.kernel == 1)   ? launch_thread_per_cell(h, P, st)
+                    : (h->opts.kernel == 3) ? launch_rounds(h, P, st)
+                                            : launch_group(h, P, st);
     if (err) return err;
   }
   if (stats) {
@@ -759,6 +891,10 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->d_boxes) cudaFree(h->d_boxes);
   if (h->h_boxes) cudaFreeHost(h->h_boxes);
   if (h->d_work) cudaFree(h->d_work);
+  if (h->d_rounds) cudaFree(h->d_rounds);
+  if (h->d_rwarp) cudaFree(h->d_rwarp);
+  if (h->d_rcnt) cudaFree(h->d_rcnt);
+  if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
   delete h;
   return 0;
 }

@@ -1,0 +1,697 @@
+// bdf_rounds.cuh -- the BDF integrator as a resumable per-cell state machine
+// whose state lives in device memory, for the round-based react path.
+//
+// Same algorithm, step for step, as the CPU oracle and the other device
+// integrators: CVODE's variable-order BDF in Nordsieck form with modified
+// Newton (reference: PelePhysics ReactorCvode denseAJ_direct, absent from
+// the snapshot; CVODE's published method).  The react call advances all
+// cells in ROUNDS; every round gives each live cell exactly one right-hand
+// side, and the cells whose Newton matrix must be rebuilt a setup:
+//
+//   rhs kernel    one THREAD per cell: f(y) for every cell of the list (all
+//                 lanes walk the same reaction at the same time);
+//   ctrl kernel   one THREAD per cell: resumes the state machine below with
+//                 that f until the cell needs its next f, a setup, or is done;
+//   setup kernel  one WARP per cell: analytic Jacobian (FP64) and the
+//                 Gauss-Jordan inverse of D (I - gamma J) D^-1 (FP32);
+//   ctrl kernel   again for the cells that were set up.
+//
+// Per-cell vectors (Nordsieck array, ewt, acor, ...) and matrices are
+// interleaved by cell ("slot"): element e of cell s at base[e * cap + s], so
+// every access of a warp of consecutive slots is one coalesced transaction.
+// The step-control scalars of a cell are one small record (RCell), loaded at
+// the start of a kernel and stored at its end.
+#pragma once
+#include "bdf_group.cuh"
+
+namespace b200 {
+namespace rounds {
+
+// Resume points of the state machine (what the cell does with its next input).
+enum Label : int {
+  kLAfterF0 = 0,   // f(y0) evaluated
+  kLAfterHin,      // f(y0 + hg y0') evaluated (initial step estimate)
+  kLAfterNStart,   // f(predicted y) evaluated: maybe setup, then Newton
+  kLAfterNIter,    // f(current Newton iterate) evaluated
+  kLAfterRestart,  // f(y) after an order-1 restart
+  kLAfterSetup,    // Newton matrix rebuilt (setup_ier holds its status)
+  // internal labels
+  kLStart, kLBeginStep, kLAttempt, kLNlsAttempt, kLNewtonIter, kLNlsRecover, kLNlsFail1, kLNlsFail2,
+  kLNlsSuccess
+};
+
+// What the cell needs next.
+enum Need : int { kNeedRhs = 0, kNeedSetup = 1, kDone = 2 };
+
+// Step-control record of one cell (doubles first, then ints).
+struct RCell {
+  double tau[kZn + 2], tq[6], l[kZn];
+  double h, hprime, hscale, eta, etamax, tn, gamma, gammap, gamrat, crate, acnrm, rl1, saved_tq5, gamma_lu;
+  double dt, saved_t, delp, hg, hub, hlb;
+  int q, qprime, L, qwait, nstlp, nstlj, jcur, ncf, nef, nflag, convfail, callSetup, jbad, mnewt, attempt;
+  int count1, hnewOK, nstloc, qmax, max_steps, setup_conv, label, setup_ier;
+  CellCounters cnt;
+};
+constexpr int kRCellD = 2 * kZn + 2 + 6 + 20;  // doubles of RCell
+constexpr int kRCellI = 23 + 7;                // ints of RCell
+static_assert(sizeof(RCell) == kRCellD * 8 + kRCellI * 4, "RCell must be packed doubles then ints");
+
+// Device-memory state of one chunk of cells.
+struct RState {
+  double* vec;     // [(kZn + 7) * n][cap]: zn[0..5], ewt, acor, ftemp, fv, F, Dsc, yev
+  double* cd;      // [kRCellD][cap] RCell doubles
+  int* ci;         // [kRCellI][cap] RCell ints
+  double* J;       // [n * n][cap] Jacobian (FP64), row-major per cell
+  void* A;         // [n * n][cap] scaled inverse of the Newton matrix (LUT)
+  long long cap;   // slots of the chunk
+};
+
+// Vectors of one cell.
+template <int n>
+struct RVec {
+  double* b;  // vec + slot
+  long long cap;
+  __device__ __forceinline__ double& at(int e) const { return b[(long long)e * cap]; }
+  __device__ __forceinline__ double& zn(int j, int i) const { return at(j * n + i); }
+  __device__ __forceinline__ double& ewt(int i) const { return at((kZn + 0) * n + i); }
+  __device__ __forceinline__ double& acor(int i) const { return at((kZn + 1) * n + i); }
+  __device__ __forceinline__ double& ftemp(int i) const { return at((kZn + 2) * n + i); }
+  __device__ __forceinline__ double& fv(int i) const { return at((kZn + 3) * n + i); }
+  __device__ __forceinline__ double& F(int i) const { return at((kZn + 4) * n + i); }
+  __device__ __forceinline__ double& dsc(int i) const { return at((kZn + 5) * n + i); }
+  __device__ __forceinline__ double& yev(int i) const { return at((kZn + 6) * n + i); }
+};
+
+__device__ __forceinline__ void load_cell(RCell& c, const RState& S, long long slot) {
+  double* d = reinterpret_cast<double*>(&c);
+  int* iv = reinterpret_cast<int*>(d + kRCellD);
+#pragma unroll
+  for (int f = 0; f < kRCellD; ++f) d[f] = S.cd[(long long)f * S.cap + slot];
+#pragma unroll
+  for (int f = 0; f < kRCellI; ++f) iv[f] = S.ci[(long long)f * S.cap + slot];
+}
+
+__device__ __forceinline__ void store_cell(const RCell& c, const RState& S, long long slot) {
+  const double* d = reinterpret_cast<const double*>(&c);
+  const int* iv = reinterpret_cast<const int*>(d + kRCellD);
+#pragma unroll
+  for (int f = 0; f < kRCellD; ++f) S.cd[(long long)f * S.cap + slot] = d[f];
+#pragma unroll
+  for (int f = 0; f < kRCellI; ++f) S.ci[(long long)f * S.cap + slot] = iv[f];
+}
+
+// ---------------------------------------------------------- BDF helpers
+template <int n>
+__device__ __forceinline__ void r_rescale(RCell& c, const RVec<n>& v) {
+  double factor = c.eta;
+  for (int j = 1; j <= c.q; ++j) {
+#pragma unroll 4
+    for (int i = 0; i < n; ++i) v.zn(j, i) *= factor;
+    factor *= c.eta;
+  }
+  c.h = c.hscale * c.eta;
+  c.hscale = c.h;
+}
+
+// Nordsieck prediction zn := zn * Pascal, column by column in registers.
+template <int n>
+__device__ __forceinline__ void r_predict(RCell& c, const RVec<n>& v) {
+  c.tn += c.h;
+  const int q = c.q;
+#pragma unroll 2
+  for (int i = 0; i < n; ++i) {
+    double z[kZn];
+#pragma unroll
+    for (int j = 0; j < kZn; ++j) z[j] = (j <= q) ? v.zn(j, i) : 0.0;
+#pragma unroll
+    for (int k = 1; k < kZn; ++k)
+#pragma unroll
+      for (int j = kZn - 1; j >= 1; --j)
+        if (j >= k && j <= q) z[j - 1] += z[j];
+#pragma unroll
+    for (int j = 0; j < kZn - 1; ++j)
+      if (j < q) v.zn(j, i) = z[j];
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void r_restore(RCell& c, const RVec<n>& v) {
+  c.tn = c.saved_t;
+  const int q = c.q;
+#pragma unroll 2
+  for (int i = 0; i < n; ++i) {
+    double z[kZn];
+#pragma unroll
+    for (int j = 0; j < kZn; ++j) z[j] = (j <= q) ? v.zn(j, i) : 0.0;
+#pragma unroll
+    for (int k = 1; k < kZn; ++k)
+#pragma unroll
+      for (int j = kZn - 1; j >= 1; --j)
+        if (j >= k && j <= q) z[j - 1] -= z[j];
+#pragma unroll
+    for (int j = 0; j < kZn - 1; ++j)
+      if (j < q) v.zn(j, i) = z[j];
+  }
+}
+
+// WRMS norm of a vector given element-wise by get(i).
+template <int n, typename Get>
+__device__ __forceinline__ double r_wrms(const RVec<n>& v, Get get) {
+  double s = 0.0;
+#pragma unroll 4
+  for (int i = 0; i < n; ++i) {
+    const double t = get(i) * v.ewt(i);
+    s += t * t;
+  }
+  return sqrt(s / n);
+}
+
+template <int n>
+__device__ __forceinline__ void r_set_bdf(RCell& c) {
+  const int q = c.q;
+  double xi_inv = 1.0, xistar_inv = 1.0;
+  c.l[0] = c.l[1] = 1.0;
+  for (int i = 2; i <= q; ++i) c.l[i] = 0.0;
+  double alpha0 = -1.0, alpha0_hat = -1.0, hsum = c.h;
+  if (q > 1) {
+    for (int j = 2; j < q; ++j) {
+      hsum += c.tau[j - 1];
+      xi_inv = c.h / hsum;
+      alpha0 -= 1.0 / j;
+      for (int i = j; i >= 1; --i) c.l[i] += c.l[i - 1] * xi_inv;
+    }
+    alpha0 -= 1.0 / q;
+    xistar_inv = -c.l[1] - alpha0;
+    hsum += c.tau[q - 1];
+    xi_inv = c.h / hsum;
+    alpha0_hat = -c.l[1] - xi_inv;
+    for (int i = q; i >= 1; --i) c.l[i] += c.l[i - 1] * xistar_inv;
+  }
+  const double A1 = 1.0 - alpha0_hat + alpha0;
+  const double A2 = 1.0 + q * A1;
+  c.tq[2] = fabs(A1 / (alpha0 * A2));
+  c.tq[5] = fabs(A2 * xistar_inv / (c.l[q] * xi_inv));
+  if (c.qwait == 1) {
+    if (q > 1) {
+      const double C = xistar_inv / c.l[q];
+      const double A3 = alpha0 + 1.0 / q;
+      const double A4 = alpha0_hat + xi_inv;
+      const double Cpinv = (1.0 - A4 + A3) / A3;
+      c.tq[1] = fabs(C * Cpinv);
+    } else {
+      c.tq[1] = 1.0;
+    }
+    hsum += c.tau[q];
+    xi_inv = c.h / hsum;
+    const double A5 = alpha0 - 1.0 / (q + 1);
+    const double A6 = alpha0_hat - xi_inv;
+    const double Cppinv = (1.0 - A6 + A5) / A2;
+    c.tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+  }
+  c.tq[4] = kNLSCOEF / c.tq[2];
+  c.rl1 = 1.0 / c.l[1];
+  c.gamma = c.h * c.rl1;
+  if (c.cnt.nst == 0) c.gammap = c.gamma;
+  c.gamrat = (c.cnt.nst > 0) ? c.gamma / c.gammap : 1.0;
+}
+
+template <int n>
+__device__ __forceinline__ void r_increase(RCell& c, const RVec<n>& v) {
+  const int q = c.q;
+  for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
+  double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = c.hscale;
+  c.l[2] = 1.0;
+  for (int j = 1; j < q; ++j) {
+    hsum += c.tau[j + 1];
+    const double xi = hsum / c.hscale;
+    prod *= xi;
+    alpha0 -= 1.0 / (j + 1);
+    alpha1 += 1.0 / xi;
+    for (int i = j + 2; i >= 2; --i) c.l[i] = c.l[i] * xiold + c.l[i - 1];
+    xiold = xi;
+  }
+  const double A1 = (-alpha0 - alpha1) / prod;
+#pragma unroll 2
+  for (int i = 0; i < n; ++i) {
+    const double z = A1 * v.zn(c.qmax, i);
+    v.zn(q + 1, i) = z;
+    for (int j = 2; j <= q; ++j) v.zn(j, i) += c.l[j] * z;
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void r_decrease(RCell& c, const RVec<n>& v) {
+  const int q = c.q;
+  for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
+  c.l[2] = 1.0;
+  double hsum = 0.0;
+  for (int j = 1; j <= q - 2; ++j) {
+    hsum += c.tau[j];
+    const double xi = hsum / c.hscale;
+    for (int i = j + 2; i >= 2; --i) c.l[i] = c.l[i] * xi + c.l[i - 1];
+  }
+#pragma unroll 2
+  for (int i = 0; i < n; ++i) {
+    const double zq = v.zn(q, i);
+    for (int j = 2; j < q; ++j) v.zn(j, i) -= c.l[j] * zq;
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void r_set_ewt(const RVec<n>& v, const double* atolv, double rtol) {
+#pragma unroll 4
+  for (int i = 0; i < n; ++i) v.ewt(i) = 1.0 / (rtol * fabs(v.zn(0, i)) + __ldg(atolv + i));
+}
+
+template <int n>
+__device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, double dsm) {
+  if (c.etamax == 1.0) {
+    c.qwait = c.qwait > 2 ? c.qwait : 2;
+    c.qprime = c.q;
+    c.hprime = c.h;
+    c.eta = 1.0;
+    return;
+  }
+  const double etaq = 1.0 / (pow(kBIAS2 * dsm, 1.0 / c.L) + kADDON);
+  if (c.qwait != 0) {
+    c.eta = etaq;
+    c.qprime = c.q;
+  } else {
+    c.qwait = 2;
+    double etaqm1 = 0.0, etaqp1 = 0.0;
+    if (c.q > 1) {
+      const int q = c.q;
+      const double ddn = r_wrms<n>(v, [&](int i) { return v.zn(q, i); }) * c.tq[1];
+      etaqm1 = 1.0 / (pow(kBIAS1 * ddn, 1.0 / c.q) + kADDON);
+    }
+    if (c.q != c.qmax && c.saved_tq5 != 0.0) {
+      const double cquot = (c.tq[5] / c.saved_tq5) * pow(c.h / c.tau[2], (double)c.L);
+      const int qm = c.qmax;
+      const double dup = r_wrms<n>(v, [&](int i) { return v.acor(i) - cquot * v.zn(qm, i); }) * c.tq[3];
+      etaqp1 = 1.0 / (pow(kBIAS3 * dup, 1.0 / (c.L + 1)) + kADDON);
+    }
+    const double etam = fmax(etaqm1, fmax(etaq, etaqp1));
+    if (etam < kTHRESH) {
+      c.eta = 1.0;
+      c.qprime = c.q;
+    } else if (etam == etaq) {
+      c.eta = etaq;
+      c.qprime = c.q;
+    } else if (etam == etaqm1) {
+      c.eta = etaqm1;
+      c.qprime = c.q - 1;
+    } else {
+      c.eta = etaqp1;
+      c.qprime = c.q + 1;
+#pragma unroll 4
+      for (int i = 0; i < n; ++i) v.zn(c.qmax, i) = v.acor(i);
+    }
+  }
+  if (c.eta < kTHRESH) {
+    c.eta = 1.0;
+    c.hprime = c.h;
+  } else {
+    c.eta = fmin(c.eta, c.etamax);
+    c.hprime = c.h * c.eta;
+  }
+}
+
+// x := D^-1 A D x with the scaled inverse A (interleaved, element (i,j) at
+// A[(i n + j) cap]); LUT = double: A is the plain inverse (no scaling).
+template <int n, typename LUT>
+__device__ __forceinline__ void r_apply_inverse(const LUT* A, long long cap, const RVec<n>& v, double (&x)[n]) {
+  constexpr bool kScaled = sizeof(LUT) == 4;
+  LUT b[n];
+#pragma unroll
+  for (int j = 0; j < n; ++j) b[j] = (LUT)(kScaled ? x[j] * v.dsc(j) : x[j]);
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    LUT acc = (LUT)0;
+#pragma unroll
+    for (int j = 0; j < n; ++j) acc += A[(long long)(i * n + j) * cap] * b[j];
+    x[i] = kScaled ? (double)acc / v.dsc(i) : (double)acc;
+  }
+}
+
+// Advance the cell from resume point `lab` until it needs a right-hand side
+// at v.yev (returns kNeedRhs with c.label set to the label that consumes it),
+// a setup (kNeedSetup), or is finished (kDone, *status set).
+template <int n, typename LUT>
+__device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
+                                         const double* J, const LUT* A, long long cap, int* status) {
+  for (int guard = 0; guard < 256; ++guard) {
+    switch (lab) {
+      case kLAfterF0: {
+        bool bad = false;
+        double hinv = 0.0;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) {
+          const double f = v.fv(i);
+          v.zn(1, i) = f;
+          bad |= !isfinite(f);
+          hinv = fmax(hinv, fabs(f) / (0.1 * fabs(v.zn(0, i)) + __ldg(atolv + i)));
+        }
+        if (bad) {
+          *status = -4;
+          return kDone;
+        }
+        const double tdist = fabs(c.dt);
+        const double tround = kUROUND * fabs(c.dt);
+        c.hlb = 100.0 * tround;
+        c.hub = 0.1 * tdist;
+        if (c.hub * hinv > 1.0) c.hub = 1.0 / hinv;
+        c.hg = sqrt(c.hlb * c.hub);
+        if (c.hub < c.hlb) {
+          c.h = c.hg;  // initial step is the geometric mean
+          c.count1 = -1;
+          lab = kLStart;
+          break;
+        }
+        c.count1 = 1;
+        c.hnewOK = 0;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + c.hg * v.zn(1, i);
+        c.label = kLAfterHin;
+        return kNeedRhs;
+      }
+      case kLAfterHin: {
+        const double hg = c.hg;
+        const double yddnrm = r_wrms<n>(v, [&](int i) { return (v.fv(i) - v.zn(1, i)) / hg; });
+        const double hnew = (yddnrm * c.hub * c.hub > 2.0) ? sqrt(2.0 / yddnrm) : sqrt(c.hg * c.hub);
+        bool stop = false;
+        if (c.hnewOK) {
+          c.hg = hnew;
+          stop = true;
+        } else {
+          const double hrat = hnew / c.hg;
+          double hn = hnew;
+          if (hrat > 0.5 && hrat < 2.0) c.hnewOK = 1;
+          if (c.count1 > 1 && hrat > 2.0) {
+            hn = c.hg;
+            c.hnewOK = 1;
+          }
+          c.hg = hn;
+          c.count1++;
+          if (c.count1 > 4) stop = true;
+        }
+        if (!stop) {
+#pragma unroll 4
+          for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + c.hg * v.zn(1, i);
+          c.label = kLAfterHin;
+          return kNeedRhs;
+        }
+        double h0 = 0.5 * c.hg;
+        if (h0 < c.hlb) h0 = c.hlb;
+        if (h0 > c.hub) h0 = c.hub;
+        c.h = h0;
+        c.count1 = -1;
+        lab = kLStart;
+        break;
+      }
+      case kLStart: {
+        const double h0 = c.h;
+        c.hscale = c.hprime = h0;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.zn(1, i) *= h0;
+        c.nstloc = 0;
+        lab = kLBeginStep;
+        break;
+      }
+      case kLBeginStep: {
+        if (c.cnt.nst > 0) r_set_ewt<n>(v, atolv, rtol);
+        if (c.nstloc >= c.max_steps) {
+          *status = -1;
+          return kDone;
+        }
+        c.saved_t = c.tn;
+        c.ncf = c.nef = 0;
+        c.nflag = kFirstCall;
+        if (c.cnt.nst > 0 && c.hprime != c.h) {
+          if (c.qprime != c.q) {
+            if (c.qprime - c.q == 1) r_increase<n>(c, v);
+            else if (c.qprime - c.q == -1) r_decrease<n>(c, v);
+            c.q = c.qprime;
+            c.L = c.q + 1;
+            c.qwait = c.L;
+          }
+          r_rescale<n>(c, v);
+        }
+        lab = kLAttempt;
+        break;
+      }
+      case kLAttempt: {
+        r_predict<n>(c, v);
+        r_set_bdf<n>(c);
+        c.convfail = (c.nflag == kFirstCall || c.nflag == kPrevErrFail) ? kNoFailures : kFailOther;
+        c.callSetup = (c.nflag == kPrevConvFail) || (c.nflag == kPrevErrFail) || (c.cnt.nst == 0) ||
+                      (c.cnt.nst >= c.nstlp + kMSBP) || (fabs(c.gamrat - 1.0) > kDGMAX_LSETUP);
+        c.jbad = 0;
+        c.attempt = 0;
+        lab = kLNlsAttempt;
+        break;
+      }
+      case kLNlsAttempt: {
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) {
+          v.acor(i) = 0.0;
+          v.yev(i) = v.zn(0, i);
+        }
+        c.label = kLAfterNStart;
+        return kNeedRhs;
+      }
+      case kLAfterNStart: {
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.ftemp(i) = v.fv(i);
+        if (c.callSetup) {
+          c.setup_conv = c.jbad ? kFailBadJ : c.convfail;
+          c.label = kLAfterSetup;
+          return kNeedSetup;
+        }
+        c.mnewt = 0;
+        c.delp = 0.0;
+        lab = kLNewtonIter;
+        break;
+      }
+      case kLAfterSetup: {
+        c.callSetup = 0;
+        if (c.setup_ier) {
+          lab = kLNlsFail2;
+          break;
+        }
+        c.mnewt = 0;
+        c.delp = 0.0;
+        lab = kLNewtonIter;
+        break;
+      }
+      case kLNewtonIter: {
+        c.cnt.nni++;
+        double dl[n], x[n];
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+          dl[i] = -(c.rl1 * v.zn(1, i) + v.acor(i) - c.gamma * v.ftemp(i));
+          x[i] = dl[i];
+        }
+        // solve (I - gamma_lu J) x = dl: FP32 inverse + one FP64 refinement step
+        r_apply_inverse<n, LUT>(A, cap, v, x);
+        if (sizeof(LUT) == 4) {
+          double r[n];
+#pragma unroll 1
+          for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < n; ++j) s += J[(long long)(i * n + j) * cap] * x[j];
+            r[i] = dl[i] - (x[i] - c.gamma_lu * s);
+          }
+          r_apply_inverse<n, LUT>(A, cap, v, r);
+#pragma unroll
+          for (int i = 0; i < n; ++i) x[i] += r[i];
+        }
+        if (c.gamrat != 1.0) {
+          const double sc = 2.0 / (1.0 + c.gamrat);
+#pragma unroll
+          for (int i = 0; i < n; ++i) x[i] *= sc;
+        }
+        double s2 = 0.0, a2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+          const double ac = v.acor(i) + x[i];
+          v.acor(i) = ac;
+          const double w = v.ewt(i);
+          s2 += (x[i] * w) * (x[i] * w);
+          a2 += (ac * w) * (ac * w);
+        }
+        const double del = sqrt(s2 / n);
+        if (c.mnewt > 0) c.crate = fmax(kCRDOWN * c.crate, del / c.delp);
+        const double dcon = del * fmin(1.0, c.crate) / c.tq[4];
+        if (dcon <= 1.0) {
+          c.acnrm = (c.mnewt == 0) ? del : sqrt(a2 / n);
+          c.jcur = 0;
+          lab = kLNlsSuccess;
+          break;
+        }
+        if ((c.mnewt >= 1 && del > kRDIV * c.delp) || !(del == del) || c.mnewt + 1 >= kMAXCOR) {
+          lab = kLNlsRecover;
+          break;
+        }
+        c.delp = del;
+        c.mnewt++;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + v.acor(i);
+        c.label = kLAfterNIter;
+        return kNeedRhs;
+      }
+      case kLAfterNIter: {
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.ftemp(i) = v.fv(i);
+        lab = kLNewtonIter;
+        break;
+      }
+      case kLNlsRecover: {
+        if (!c.jcur && c.attempt < 3) {
+          c.callSetup = 1;
+          c.jbad = 1;
+          c.attempt++;
+          lab = kLNlsAttempt;
+          break;
+        }
+        lab = kLNlsFail1;
+        break;
+      }
+      case kLNlsFail1:
+      case kLNlsFail2: {
+        c.cnt.ncfn++;
+        r_restore<n>(c, v);
+        c.ncf++;
+        c.etamax = 1.0;
+        if (c.ncf == kMXNCF) {
+          *status = (lab == kLNlsFail2) ? -5 : -3;
+          return kDone;
+        }
+        c.eta = kETACF;
+        c.nflag = kPrevConvFail;
+        r_rescale<n>(c, v);
+        lab = kLAttempt;
+        break;
+      }
+      case kLNlsSuccess: {
+        const double dsm = c.acnrm * c.tq[2];
+        if (dsm <= 1.0) {
+          // complete the step
+          c.cnt.nst++;
+          for (int i = c.q; i >= 2; --i) c.tau[i] = c.tau[i - 1];
+          if (c.q == 1 && c.cnt.nst > 1) c.tau[2] = c.tau[1];
+          c.tau[1] = c.h;
+          const int q = c.q;
+          const bool save = (c.qwait - 1 == 1 && q != c.qmax);
+#pragma unroll 2
+          for (int i = 0; i < n; ++i) {
+            const double ac = v.acor(i);
+            for (int j = 0; j <= q; ++j) v.zn(j, i) += c.l[j] * ac;
+            if (save) v.zn(c.qmax, i) = ac;
+          }
+          c.qwait--;
+          if (save) c.saved_tq5 = c.tq[5];
+          r_prepare_next<n>(c, v, dsm);
+          c.etamax = (c.cnt.nst <= kSMALL_NST) ? kETAMX2 : kETAMX3;
+          c.nstloc++;
+          if (c.tn - c.dt >= 0.0) {
+            *status = 0;
+            return kDone;
+          }
+          lab = kLBeginStep;
+          break;
+        }
+        c.nef++;
+        c.cnt.netf++;
+        c.nflag = kPrevErrFail;
+        r_restore<n>(c, v);
+        if (c.nef == kMXNEF) {
+          *status = -2;
+          return kDone;
+        }
+        c.etamax = 1.0;
+        if (c.nef <= kMXNEF1) {
+          c.eta = 1.0 / (pow(kBIAS2 * dsm, 1.0 / c.L) + kADDON);
+          c.eta = fmax(kETAMIN, c.eta);
+          if (c.nef >= kSMALL_NEF) c.eta = fmin(c.eta, kETAMXF);
+          r_rescale<n>(c, v);
+          lab = kLAttempt;
+          break;
+        }
+        if (c.q > 1) {
+          c.eta = kETAMIN;
+          r_decrease<n>(c, v);
+          c.L = c.q;
+          c.q--;
+          c.qwait = c.L;
+          r_rescale<n>(c, v);
+          lab = kLAttempt;
+          break;
+        }
+        c.eta = kETAMIN;
+        c.h *= c.eta;
+        c.hscale = c.h;
+        c.qwait = kLONG_WAIT;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i);
+        c.label = kLAfterRestart;
+        return kNeedRhs;
+      }
+      case kLAfterRestart: {
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) v.zn(1, i) = c.h * v.fv(i);
+        lab = kLAttempt;
+        break;
+      }
+      default:
+        *status = -3;
+        return kDone;
+    }
+  }
+  *status = -3;  // the state machine never loops this long without an RHS
+  return kDone;
+}
+
+// Start a cell whose zn[0] (state) and F (forcing) are loaded: counters and
+// step-control defaults, then ask for f(y0).
+template <int n>
+__device__ __forceinline__ void r_begin(RCell& c, const RVec<n>& v, const double* atolv, double rtol, double dt,
+                                        int qmax, int max_steps) {
+  c.tn = 0.0;
+  c.dt = dt;
+  c.cnt = CellCounters{0, 0, 0, 0, 0, 0, 0};
+  c.nstlp = c.nstlj = 0;
+  c.q = c.qprime = 1;
+  c.L = 2;
+  c.qwait = c.L;
+  c.etamax = kETAMX1;
+  c.saved_tq5 = 0.0;
+  c.crate = 1.0;
+  c.jcur = 0;
+  c.gammap = c.gamma = 1.0;
+  c.gamrat = 1.0;
+  c.gamma_lu = 1.0;
+  c.qmax = qmax;
+  c.max_steps = max_steps;
+  c.h = c.hprime = c.hscale = c.eta = 1.0;
+  c.acnrm = c.rl1 = c.saved_t = c.delp = c.hg = c.hub = c.hlb = 0.0;
+  c.ncf = c.nef = c.nflag = c.convfail = c.callSetup = c.jbad = c.mnewt = c.attempt = 0;
+  c.count1 = c.hnewOK = c.nstloc = c.setup_conv = c.setup_ier = 0;
+#pragma unroll
+  for (int i = 0; i < kZn + 2; ++i) c.tau[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) c.tq[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < kZn; ++i) c.l[i] = 0.0;
+#pragma unroll 2
+  for (int i = 0; i < n; ++i) {
+    for (int j = 1; j < kZn; ++j) v.zn(j, i) = 0.0;
+    v.acor(i) = 0.0;
+    v.yev(i) = v.zn(0, i);
+  }
+  r_set_ewt<n>(v, atolv, rtol);
+  c.label = kLAfterF0;
+}
+
+}  // namespace rounds
+}  // namespace b200

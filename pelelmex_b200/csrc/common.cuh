@@ -6,6 +6,7 @@
 
 #include "../../include/b200chem.h"
 #include "bdf_group.cuh"
+#include "bdf_rounds.cuh"
 
 namespace b200 {
 
@@ -106,5 +107,46 @@ bool tpc_supported(int N);
 cudaError_t tpc_occupancy(int N, int lut_bytes, int* per_sm, int* smem);
 cudaError_t tpc_launch(int N, int lut_bytes, const ReactParams& P, const TpcParams& Q, int grid, int smem,
                        cudaStream_t st);
+
+// ------------------------------------------------------ round-based path
+constexpr int kRoundsRhsBlock = 64;  // threads per CTA of the rhs kernel
+enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsSetup };
+
+// Per-warp scratch of the setup kernel.  Shared: C, g/RT, h/RT, Dsc [Npad]
+// (double), rates [Rpad] (double), inverse [n][ldl] + pivot column [Npad]
+// (LUT), pivots [n] (int).  Global: column-major Jacobian [n][ldj] and four
+// per-reaction arrays [Rpad] (double).
+struct RoundsSetupLayout {
+  int Npad, Rpad, ldj, ldl;
+  int smem_per_warp;
+  long long gbytes_per_warp;
+};
+
+struct RoundsParams {
+  ReactParams P;
+  rounds::RState S;
+  RoundsSetupLayout SL;
+  long long chunk0;  // first cell of the chunk (index into the react call's cells)
+  long long nchunk;  // cells in the chunk
+  const int* list_in;
+  const int* cnt_in;
+  int* list_out;     // cells that need a right-hand side next round
+  int* cnt_out;
+  int* list_setup;   // cells that need a Newton-matrix setup this round
+  int* cnt_setup;
+  unsigned char* wscratch;  // [setup warps][SL.gbytes_per_warp]
+};
+
+struct RoundsGrids {
+  int start, rhs, ctrl, setup;
+};
+
+bool rounds_supported(int N);
+RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes);
+long long rounds_state_bytes_per_cell(int N, int lut_bytes);
+rounds::RState rounds_carve(void* base, long long cap, int N, int lut_bytes);
+cudaError_t rounds_grids_for(int N, int lut_bytes, const RoundsSetupLayout& SL, int sm_count, RoundsGrids* G);
+cudaError_t rounds_launch(int N, int lut_bytes, int what, const RoundsParams& R, const RoundsGrids& G, int after_rhs,
+                          cudaStream_t st);
 
 }  // namespace b200

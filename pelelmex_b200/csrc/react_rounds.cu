@@ -1,0 +1,556 @@
+// react_rounds.cu -- round-based react path: rhs / ctrl / setup kernels over
+// compacted cell lists, and their host-side launch sequence.
+//
+// A react call is processed in chunks of cells (as many as the state buffer
+// holds).  For one chunk:
+//   start                     load every cell, mask / validity checks, list A
+//   repeat until A is empty:
+//     rhs   (A)               f(y) for every cell of A (thread per cell)
+//     ctrl  (A -> B, S)       resume each cell with its f: next f -> B,
+//                             Newton-matrix setup -> S, finished -> outputs
+//     setup (S)               Jacobian + inverse (warp per cell)
+//     ctrl  (S -> B)          resume the set-up cells
+//     swap A, B
+// Lists are appended with warp-aggregated atomics, so a warp's slots stay in
+// order and the interleaved state accesses stay coalesced as cells drop out.
+#include <algorithm>
+
+#include "bdf_rounds.cuh"
+#include "common.cuh"
+
+namespace b200 {
+using namespace rounds;
+
+namespace {
+
+// (box, i, j, k) of a global cell index of the react call.
+struct CellLoc {
+  const DevBox* bx;
+  int i, j, k;
+};
+
+__device__ __forceinline__ CellLoc locate(const ReactParams& P, long long cell) {
+  int lo = 0, hi = P.nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (P.boxes[mid].off <= cell) lo = mid;
+    else hi = mid - 1;
+  }
+  CellLoc L;
+  L.bx = P.boxes + lo;
+  const long long loc = cell - L.bx->off;
+  L.i = L.bx->lo0 + (int)(loc % L.bx->nx);
+  L.j = L.bx->lo1 + (int)((loc / L.bx->nx) % L.bx->ny);
+  L.k = L.bx->lo2 + (int)(loc / ((long long)L.bx->nx * L.bx->ny));
+  return L;
+}
+
+// Append `val` to list/cnt for the lanes with pred (all 32 lanes call it).
+__device__ __forceinline__ void warp_append(bool pred, int val, int* list, int* cnt) {
+  const unsigned m = __ballot_sync(kFull, pred);
+  if (m == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(cnt, __popc(m));
+  base = __shfl_sync(kFull, base, leader);
+  if (pred) list[base + __popc(m & ((1u << lane) - 1u))] = val;
+}
+
+// Warp-aggregated statistics of the lanes with `done` (all 32 lanes call it).
+__device__ __forceinline__ void warp_stats(long long* stats, bool done, bool failed, bool masked,
+                                           const CellCounters& cnt) {
+  if (!stats || __ballot_sync(kFull, done || masked) == 0) return;
+  long long v[kStMaxNfe];
+  v[kStCells] = done;
+  v[kStMasked] = masked;
+  v[kStFailed] = done && failed;
+  v[kStNst] = done ? cnt.nst : 0;
+  v[kStNfe] = done ? cnt.nfe : 0;
+  v[kStNje] = done ? cnt.nje : 0;
+  v[kStNlu] = done ? cnt.nlu : 0;
+  v[kStNetf] = done ? cnt.netf : 0;
+  v[kStNcfn] = done ? cnt.ncfn : 0;
+  long long mx = done ? cnt.nfe : 0, ms = done ? cnt.nst : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int s = 0; s < kStMaxNfe; ++s) v[s] += __shfl_xor_sync(kFull, v[s], o);
+    mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    ms = max(ms, __shfl_xor_sync(kFull, ms, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int s = 0; s < kStMaxNfe; ++s)
+      if (v[s]) atomicAdd(reinterpret_cast<unsigned long long*>(stats + s), (unsigned long long)v[s]);
+    if (mx) atomicMax(stats + kStMaxNfe, mx);
+    if (ms) atomicMax(stats + kStMaxNst, ms);
+  }
+}
+
+// ------------------------------------------------------------ mechanism
+// One reaction's rate of progress for the thread's cell; C, g/RT per thread
+// in shared memory at [k * ss].  Every thread of the warp evaluates the SAME
+// reaction j, so the table reads are broadcasts and the branches uniform.
+__device__ __forceinline__ double r_progress(const DevMech& m, int j, double T, double lnT, double invT,
+                                             double Ctot, double lnPRT, const double* sC, const double* sG,
+                                             int ss) {
+  const int R = m.R;
+  const double lnA = __ldg(m.arr + j), b = __ldg(m.arr + R + j), ea = __ldg(m.arr + 2 * R + j);
+  const double kinf = exp(lnA + b * lnT - ea * invT);
+  const int type = __ldg(m.rtype + j);
+  const int flags = __ldg(m.rflags + j);
+  double M = 0.0;
+  if (type != 0) {
+    M = Ctot;
+    const int e0 = __ldg(m.eff_ptr + j), e1 = __ldg(m.eff_ptr + j + 1);
+    for (int q = e0; q < e1; ++q) M += __ldg(m.eff_m1 + q) * sC[__ldg(m.eff_sp + q) * ss];
+  }
+  double kf = kinf;
+  if (type >= 2) {
+    const double lnA0 = __ldg(m.arr_lo + j), b0 = __ldg(m.arr_lo + R + j), ea0 = __ldg(m.arr_lo + 2 * R + j);
+    const double k0 = exp(lnA0 + b0 * lnT - ea0 * invT);
+    const double Pr = k0 * M / kinf;
+    double F = 1.0;
+    if (type == 3) {
+      const double a = __ldg(m.troe + j), i3 = __ldg(m.troe + R + j), i1 = __ldg(m.troe + 2 * R + j);
+      const double t2 = __ldg(m.troe + 3 * R + j);
+      double Fc = (1.0 - a) * exp(-T * i3) + a * exp(-T * i1);
+      if (flags & 4) Fc += exp(-t2 * invT);
+      const double logFc = log10(fmax(Fc, 1e-300));
+      const double c = -0.4 - 0.67 * logFc, nn = 0.75 - 1.27 * logFc;
+      const double u = log10(fmax(Pr, 1e-300)) + c;
+      const double f1 = u / (nn - 0.14 * u);
+      F = exp(kLn10 * (logFc / (1.0 + f1 * f1)));
+    }
+    kf = kinf * Pr / (1.0 + Pr) * F;
+  }
+  // slots 0..3 reactants (nu < 0), 4..7 products (nu > 0)
+  double pf = 1.0, pr = 1.0, sg = 0.0;
+#pragma unroll
+  for (int sl = 0; sl < 8; ++sl) {
+    const int k = __ldg(m.sp + sl * R + j);
+    if (k >= 0) {
+      const int nu = __ldg(m.nu + sl * R + j);
+      const int na = nu < 0 ? -nu : nu;
+      const double ck = sC[k * ss];
+      double p = ck;
+      for (int e = 1; e < na; ++e) p *= ck;
+      if (sl < 4) pf *= p;
+      else pr *= p;
+      sg += nu * sG[k * ss];
+    }
+  }
+  double kr = 0.0;
+  if (flags & 2) {
+    const double lr = __ldg(m.arr_rev + j), br = __ldg(m.arr_rev + R + j), er = __ldg(m.arr_rev + 2 * R + j);
+    kr = exp(lr + br * lnT - er * invT);
+  } else if (flags & 1) {
+    kr = kf * exp(sg - __ldg(m.sdnu + j) * lnPRT);
+  }
+  double q = kf * pf - kr * pr;
+  if (type == 1) q *= M;
+  return q;
+}
+
+// HP right-hand side at v.yev (forcing v.F) into v.fv, thread per cell.
+template <int NS>
+__device__ __forceinline__ void r_rhs(const DevMech& m, const RVec<NS + 1>& v, double* sC, double* sG, double* sW,
+                                      int ss) {
+  const double T = v.yev(NS);
+  const double lnT = log(T), invT = 1.0 / T;
+  double Ctot = 0.0, rcp = 0.0;
+#pragma unroll 1
+  for (int k = 0; k < NS; ++k) {
+    double cpR, hRT, sR, dcpR;
+    nasa7(m, k, T, lnT, cpR, hRT, sR, dcpR);
+    const double iw = __ldg(m.inv_mw + k);
+    const double yk = v.yev(k);
+    const double Ck = yk * iw;
+    sC[k * ss] = Ck;
+    sG[k * ss] = hRT - sR;
+    sW[k * ss] = 0.0;
+    Ctot += Ck;
+    rcp += yk * cpR * kRu * iw;
+  }
+  const double lnPRT = log(kPatm / (kRu * T));
+  const int R = m.R;
+#pragma unroll 1
+  for (int j = 0; j < R; ++j) {
+    const double q = r_progress(m, j, T, lnT, invT, Ctot, lnPRT, sC, sG, ss);
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+      const int k = __ldg(m.sp + sl * R + j);
+      if (k >= 0) {
+        sW[k * ss] += (double)__ldg(m.nu + sl * R + j) * q;
+      }
+    }
+  }
+  double hs = 0.0;
+#pragma unroll 1
+  for (int k = 0; k < NS; ++k) {
+    double cpR, hRT, sR, dcpR;
+    nasa7(m, k, T, lnT, cpR, hRT, sR, dcpR);
+    const double yd = sW[k * ss] * __ldg(m.mw + k) + v.F(k);
+    v.fv(k) = yd;
+    hs += hRT * kRu * T * __ldg(m.inv_mw + k) * yd;
+  }
+  v.fv(NS) = (v.F(NS) - hs) / rcp;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- kernels
+template <int NS>
+__global__ void __launch_bounds__(128) rk_start(RoundsParams R) {
+  constexpr int n = NS + 1;
+  const ReactParams& P = R.P;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < R.nchunk; base += stride) {
+    const long long slot = base + threadIdx.x;
+    const bool live = slot < R.nchunk;
+    bool go = false, done = false, masked = false;
+    if (live) {
+      const long long cell = R.chunk0 + slot;
+      const CellLoc L = locate(P, cell);
+      const DevBox& bx = *L.bx;
+      if (bx.mask.p)
+        masked = bx.mask.p[(long long)(L.i - bx.mask.lo0) + (long long)(L.j - bx.mask.lo1) * bx.mask.js +
+                           (long long)(L.k - bx.mask.lo2) * bx.mask.ks] == 0;
+      int code = 0;
+      if (masked) {
+        code = B200CHEM_CELL_MASKED;
+        if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = 0.0;
+      } else {
+        const RVec<n> v{R.S.vec + slot, R.S.cap};
+        const double* yp = elem(bx.rhoY, L.i, L.j, L.k);
+        const double* fp = elem(bx.fY, L.i, L.j, L.k);
+        double rho = 0.0;
+        bool bad = false;
+#pragma unroll 4
+        for (int q = 0; q < NS; ++q) {
+          const double y = yp[q * bx.rhoY.ns], f = fp[q * bx.fY.ns];
+          v.zn(0, q) = y;
+          v.F(q) = f;
+          rho += y;
+          bad |= !isfinite(y) || !isfinite(f);
+        }
+        const double T = *elem(bx.T, L.i, L.j, L.k), fH = *elem(bx.fH, L.i, L.j, L.k);
+        v.zn(0, NS) = T;
+        v.F(NS) = fH;
+        bad |= !(T > 0.0) || !isfinite(T) || !isfinite(fH) || !(rho > 0.0);
+        if (bad) {
+          code = B200CHEM_CELL_NONFINITE;
+          if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = 0.0;
+          done = true;
+        } else {
+          RCell c;
+          r_begin<n>(c, v, P.atol, P.rtol, P.dt, P.qmax, P.max_steps);
+          store_cell(c, R.S, slot);
+          go = true;
+        }
+      }
+      if (!go && P.status) P.status[cell] = code;
+    }
+    warp_append(go, (int)slot, R.list_out, R.cnt_out);
+    warp_stats(P.stats, done, true, masked, CellCounters{0, 0, 0, 0, 0, 0, 0});
+  }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
+  constexpr int n = NS + 1;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ DevMech s_mech;
+  if (threadIdx.x == 0) s_mech = R.P.mech;
+  __syncthreads();
+  const int cnt = *R.cnt_in;
+  double* sC = reinterpret_cast<double*>(dsm) + threadIdx.x;
+  double* sG = sC + NS * blockDim.x;
+  double* sW = sG + NS * blockDim.x;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
+    const int slot = R.list_in[idx];
+    const RVec<n> v{R.S.vec + slot, R.S.cap};
+    r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
+  }
+}
+
+// Resume the cells of list_in.  after_rhs: each consumes the f just
+// evaluated (counted in nfe); otherwise they come back from a setup.
+template <int NS, typename LUT>
+__global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
+  constexpr int n = NS + 1;
+  const ReactParams& P = R.P;
+  const int cnt = *R.cnt_in;
+  const LUT* Abase = reinterpret_cast<const LUT*>(R.S.A);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < cnt; base += stride) {
+    const int idx = base + threadIdx.x;
+    const bool live = idx < cnt;
+    int slot = 0, need = kDone, status = 0;
+    RCell c;
+    if (live) {
+      slot = R.list_in[idx];
+      load_cell(c, R.S, slot);
+      if (after_rhs) c.cnt.nfe++;
+      const RVec<n> v{R.S.vec + slot, R.S.cap};
+      need = r_advance<n, LUT>(c, v, c.label, P.atol, P.rtol, R.S.J + slot, Abase + slot, R.S.cap, &status);
+      store_cell(c, R.S, slot);
+      if (need == kDone) {
+        const long long cell = R.chunk0 + slot;
+        const CellLoc L = locate(P, cell);
+        const DevBox& bx = *L.bx;
+        if (status == 0) {
+          // y(dt) from the Nordsieck array (Horner in s = (dt - tn) / h)
+          const double s = (P.dt - c.tn) / c.h;
+          double* yp = elem(bx.rhoY, L.i, L.j, L.k);
+#pragma unroll 2
+          for (int q = 0; q < n; ++q) {
+            double y = v.zn(c.q, q);
+            for (int jj = c.q - 1; jj >= 0; --jj) y = v.zn(jj, q) + s * y;
+            if (q < NS) yp[q * bx.rhoY.ns] = y;
+            else *elem(bx.T, L.i, L.j, L.k) = y;
+          }
+          double* hp = elem(bx.rhoH, L.i, L.j, L.k);
+          *hp = *hp + P.dt * v.F(NS);
+        }
+        if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
+        if (P.status) P.status[cell] = status;
+      }
+    }
+    warp_append(live && need == kNeedRhs, slot, R.list_out, R.cnt_out);
+    warp_append(live && need == kNeedSetup, slot, R.list_setup, R.cnt_setup);
+    warp_stats(P.stats, live && need == kDone, status != 0, false, c.cnt);
+  }
+}
+
+// Newton-matrix setup, one warp per cell: maybe a fresh analytic Jacobian
+// (CVODE's jbad rule), then the Gauss-Jordan inverse of D (I - gamma J) D^-1.
+template <int NS, typename LUT, int CPL>
+__global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
+  constexpr int n = NS + 1;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ DevMech s_mech;
+  if (threadIdx.x == 0) s_mech = R.P.mech;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const RoundsSetupLayout& SL = R.SL;
+  // per-warp shared scratch
+  unsigned char* sb = dsm + (size_t)w * SL.smem_per_warp;
+  double* d = reinterpret_cast<double*>(sb);
+  GrpScratch ms;
+  ms.C = d;
+  ms.gRT = d + SL.Npad;
+  ms.hRT = d + 2 * SL.Npad;
+  double* Dsc = d + 3 * SL.Npad;
+  ms.q = d + 4 * SL.Npad;
+  LUT* A = reinterpret_cast<LUT*>(ms.q + SL.Rpad);
+  LUT* fcol = A + (size_t)n * SL.ldl;
+  int* ipiv = reinterpret_cast<int*>(fcol + SL.Npad);
+  // per-warp global scratch: column-major Jacobian and per-reaction terms
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
+  double* Jw = reinterpret_cast<double*>(R.wscratch + gw * SL.gbytes_per_warp);
+  ms.r1 = Jw + (size_t)n * SL.ldj;
+  ms.r2 = ms.r1 + SL.Rpad;
+  ms.r3 = ms.r2 + SL.Rpad;
+  ms.r4 = ms.r3 + SL.Rpad;
+  const int cnt = *R.cnt_in;
+  const long long cap = R.S.cap;
+  LUT* Ag = reinterpret_cast<LUT*>(R.S.A);
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long idx = gw; idx < cnt; idx += nwarps) {
+    const int slot = R.list_in[idx];
+    const RVec<n> v{R.S.vec + slot, cap};
+    RCell c;
+    load_cell(c, R.S, slot);
+    const double dgamma = fabs(c.gamma / c.gammap - 1.0);
+    const bool jbad = (c.cnt.nst == 0) || (c.cnt.nst >= c.nstlj + kMSBJ) ||
+                      (c.setup_conv == kFailBadJ && dgamma < kDGMAX_JBAD) || (c.setup_conv == kFailOther);
+    if (jbad) {
+      Vec<CPL> y, fy;
+#pragma unroll
+      for (int cc = 0; cc < CPL; ++cc) {
+        const int i = lane + 32 * cc;
+        y.v[cc] = (i < n) ? v.yev(i) : 0.0;
+        fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
+      }
+      grp_jac<32, CPL>(&s_mech, ms, y, fy, Jw, SL.ldj, lane);
+      __syncwarp();
+      // keep the Jacobian for the refinement step and later setups
+      for (int l = 0; l < n; ++l)
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int i = lane + 32 * cc;
+          if (i < n) R.S.J[(long long)(i * n + l) * cap + slot] = Jw[l * SL.ldj + i];
+        }
+      c.cnt.nje++;
+      c.nstlj = c.cnt.nst;
+      c.jcur = 1;
+    } else {
+      for (int l = 0; l < n; ++l)
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int i = lane + 32 * cc;
+          if (i < n) Jw[l * SL.ldj + i] = R.S.J[(long long)(i * n + l) * cap + slot];
+        }
+      c.jcur = 0;
+    }
+#pragma unroll
+    for (int cc = 0; cc < CPL; ++cc) {
+      const int i = lane + 32 * cc;
+      if (i < n) {
+        const double ds = (sizeof(LUT) == 4) ? v.ewt(i) : 1.0;
+        Dsc[i] = ds;
+        v.dsc(i) = ds;
+      }
+    }
+    __syncwarp();
+    const int ier = grp_gj_inverse<32, LUT>(Jw, SL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, c.gamma, lane);
+    __syncwarp();
+    if (ier == 0)
+      for (int i = 0; i < n; ++i)
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int j = lane + 32 * cc;
+          if (j < n) Ag[(long long)(i * n + j) * cap + slot] = A[i * SL.ldl + j];
+        }
+    c.cnt.nlu++;
+    c.gamma_lu = c.gamma;
+    c.gamrat = 1.0;
+    c.gammap = c.gamma;
+    c.crate = 1.0;
+    c.nstlp = c.cnt.nst;
+    c.setup_ier = ier;
+    if (lane == 0) store_cell(c, R.S, slot);
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ host side
+namespace {
+
+template <int NS>
+int rhs_smem(int block) { return 3 * NS * block * (int)sizeof(double); }
+
+template <int NS, typename LUT>
+cudaError_t rounds_setup_attrs(const RoundsSetupLayout& SL) {
+  constexpr int n = NS + 1;
+  constexpr int CPL = (n + 31) / 32;
+  cudaError_t e = cudaFuncSetAttribute(rk_rhs<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       rhs_smem<NS>(kRoundsRhsBlock));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rk_setup<NS, LUT, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              4 * SL.smem_per_warp);
+}
+
+template <int NS, typename LUT>
+cudaError_t rounds_grids(const RoundsSetupLayout& SL, int sm_count, RoundsGrids* G) {
+  constexpr int n = NS + 1;
+  constexpr int CPL = (n + 31) / 32;
+  cudaError_t e = rounds_setup_attrs<NS, LUT>(SL);
+  if (e != cudaSuccess) return e;
+  int b = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_rhs<NS>, kRoundsRhsBlock,
+                                                         rhs_smem<NS>(kRoundsRhsBlock))) != cudaSuccess)
+    return e;
+  G->rhs = std::max(1, b) * sm_count;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_ctrl<NS, LUT>, 128, 0)) != cudaSuccess) return e;
+  G->ctrl = std::max(1, b) * sm_count;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_setup<NS, LUT, CPL>, 128, 4 * SL.smem_per_warp)) !=
+      cudaSuccess)
+    return e;
+  G->setup = std::max(1, b) * sm_count;
+  G->start = 4 * sm_count;
+  return cudaSuccess;
+}
+
+template <int NS, typename LUT>
+cudaError_t rounds_launch_t(int what, const RoundsParams& R, const RoundsGrids& G, int after_rhs, cudaStream_t st) {
+  constexpr int n = NS + 1;
+  constexpr int CPL = (n + 31) / 32;
+  switch (what) {
+    case kRoundsStart:
+      rk_start<NS><<<G.start, 128, 0, st>>>(R);
+      break;
+    case kRoundsRhs:
+      rk_rhs<NS><<<G.rhs, kRoundsRhsBlock, rhs_smem<NS>(kRoundsRhsBlock), st>>>(R);
+      break;
+    case kRoundsCtrl:
+      rk_ctrl<NS, LUT><<<G.ctrl, 128, 0, st>>>(R, after_rhs);
+      break;
+    case kRoundsSetup:
+      rk_setup<NS, LUT, CPL><<<G.setup, 128, 4 * R.SL.smem_per_warp, st>>>(R);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+bool rounds_supported(int N) { return N == 9 || N == 21 || N == 53; }
+
+RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
+  RoundsSetupLayout L;
+  const int n = N + 1;
+  L.Npad = ((n + 31) / 32) * 32;
+  L.Rpad = std::max(32, ((R + 31) / 32) * 32);
+  L.ldj = n | 1;
+  L.ldl = n | 1;
+  long long b = 8LL * (4 * L.Npad + L.Rpad);
+  b += (long long)lut_bytes * ((long long)n * L.ldl + L.Npad);
+  b += 4LL * n;
+  L.smem_per_warp = (int)((b + 15) & ~15LL);
+  L.gbytes_per_warp = (8LL * ((long long)n * L.ldj + 4LL * L.Rpad) + 255) & ~255LL;
+  return L;
+}
+
+long long rounds_state_bytes_per_cell(int N, int lut_bytes) {
+  const long long n = N + 1;
+  return 8LL * (kZn + 7) * n + 8LL * kRCellD + 4LL * kRCellI + 8LL * n * n + (long long)lut_bytes * n * n +
+         4LL * 3;  // three slot lists
+}
+
+RState rounds_carve(void* base, long long cap, int N, int lut_bytes) {
+  const long long n = N + 1;
+  RState S;
+  unsigned char* p = static_cast<unsigned char*>(base);
+  auto take = [&](long long bytes) {
+    unsigned char* r = p;
+    p += (bytes + 255) & ~255LL;
+    return r;
+  };
+  S.vec = reinterpret_cast<double*>(take(8LL * (kZn + 7) * n * cap));
+  S.cd = reinterpret_cast<double*>(take(8LL * kRCellD * cap));
+  S.ci = reinterpret_cast<int*>(take(4LL * kRCellI * cap));
+  S.J = reinterpret_cast<double*>(take(8LL * n * n * cap));
+  S.A = take((long long)lut_bytes * n * n * cap);
+  S.cap = cap;
+  return S;
+}
+
+cudaError_t rounds_grids_for(int N, int lut_bytes, const RoundsSetupLayout& SL, int sm_count, RoundsGrids* G) {
+  if (N == 9) return lut_bytes == 4 ? rounds_grids<9, float>(SL, sm_count, G) : rounds_grids<9, double>(SL, sm_count, G);
+  if (N == 21)
+    return lut_bytes == 4 ? rounds_grids<21, float>(SL, sm_count, G) : rounds_grids<21, double>(SL, sm_count, G);
+  if (N == 53)
+    return lut_bytes == 4 ? rounds_grids<53, float>(SL, sm_count, G) : rounds_grids<53, double>(SL, sm_count, G);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t rounds_launch(int N, int lut_bytes, int what, const RoundsParams& R, const RoundsGrids& G, int after_rhs,
+                          cudaStream_t st) {
+  if (N == 9)
+    return lut_bytes == 4 ? rounds_launch_t<9, float>(what, R, G, after_rhs, st)
+                          : rounds_launch_t<9, double>(what, R, G, after_rhs, st);
+  if (N == 21)
+    return lut_bytes == 4 ? rounds_launch_t<21, float>(what, R, G, after_rhs, st)
+                          : rounds_launch_t<21, double>(what, R, G, after_rhs, st);
+  if (N == 53)
+    return lut_bytes == 4 ? rounds_launch_t<53, float>(what, R, G, after_rhs, st)
+                          : rounds_launch_t<53, double>(what, R, G, after_rhs, st);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace b200

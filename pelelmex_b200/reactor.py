@@ -104,7 +104,7 @@ class ReactorB200:
     """Batched HP reactor on one B200 (warp-per-cell BDF, persistent kernel)."""
 
     # defaults of the reference's reactor keys (Docs/sphinx/manual/LMeXControls.rst:301-310)
-    KERNELS = {"auto": 0, "thread": 1, "group": 2}
+    KERNELS = {"auto": 0, "thread": 1, "group": 2, "rounds": 3}
 
     def __init__(self, mechanism=None, rtol: float = 1e-10, atol: float = 1e-10, max_order: int = 2,
                  max_steps: int = 10000, lu_fp64: bool = False, warps_per_cta: int = 0, kernel: str = "auto",

@@ -1,0 +1,119 @@
+"""GPU parity of the round-based integrator (kernel = "rounds") against the
+CPU oracle, through the C ABI, at the reactor's parity tolerances (T within
+1e-5 relative, Y within 1e-8 absolute at rtol 1e-8 / atol 1e-12)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from pelelmex_b200 import mechanism as M, workloads as W  # noqa: E402
+from test_gpu_parity import T_RTOL, compare, orc_cache, run_gpu  # noqa: E402,F401
+
+
+def _oracle(orc_cache, name, f, **kw):
+    args = dict(rtol=1e-8, atol=1e-12, max_order=5)
+    args.update(kw)
+    return orc_cache(name).react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, **args)
+
+
+@pytest.mark.parametrize("lu_fp64", [False, True])
+def test_rounds_premixed_h2_32cubed(lu_fp64, orc_cache):
+    mech = M.builtin("synth_h2_9")
+    f = W.premixed_h2(mech, edge=32, dt=1e-6)
+    g = run_gpu("synth_h2_9", f, kernel="rounds", lu_fp64=lu_fp64)
+    o = _oracle(orc_cache, "synth_h2_9", f)
+    assert (g["status"] == 0).all() and o["nfail"] == 0
+    compare(f, g, o, f"rounds premixed_h2 32^3 lu_fp64={lu_fp64}")
+    assert np.allclose(g["rhoH"], o["rhoH"], rtol=1e-15, atol=0)
+    st = g["stats"]
+    assert st["n_cells"] == f.ncells and st["n_failed"] == 0
+    assert st["nfe"] == int(g["fct"].sum())
+
+
+@pytest.mark.parametrize("dt", [1e-6, 1e-5])
+@pytest.mark.parametrize("lu_fp64", [False, True])
+def test_rounds_flame_ch4_sample(dt, lu_fp64, orc_cache):
+    mech = M.builtin("synth_ch4_21")
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 4096), dt=dt)
+    g = run_gpu("synth_ch4_21", f, kernel="rounds", lu_fp64=lu_fp64)
+    o = _oracle(orc_cache, "synth_ch4_21", f)
+    assert (g["status"] == 0).all() and o["nfail"] == 0
+    compare(f, g, o, f"rounds flame_ch4 dt={dt} lu_fp64={lu_fp64}")
+    # same algorithm as the oracle: the per-cell work counters agree closely
+    assert abs(g["fct"].mean() - o["fct"].mean()) <= 0.02 * o["fct"].mean()
+
+
+def test_rounds_matches_group_integrator():
+    mech = M.builtin("synth_ch4_21")
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 2048, seed=21), dt=1e-5)
+    a = run_gpu("synth_ch4_21", f, kernel="rounds")
+    b = run_gpu("synth_ch4_21", f, kernel="group")
+    assert (a["status"] == 0).all() and (b["status"] == 0).all()
+    assert np.max(np.abs(a["T"] - b["T"]) / b["T"]) <= T_RTOL
+    rho = f.rhoY.sum(axis=0)
+    assert (np.abs(a["rhoY"] - b["rhoY"]).max(axis=0) / rho).max() <= 1e-8
+
+
+def test_rounds_dodecane(orc_cache):
+    mech = M.builtin("synth_c12_53")
+    rng = np.random.default_rng(7)
+    nm = mech.names
+    n = 256
+    X = np.zeros((n, mech.n_species))
+    X[:, nm.index("NC12H26")] = rng.uniform(0.5, 2.0, n)
+    X[:, nm.index("O2")] = 18.5
+    X[:, nm.index("N2")] = 69.6
+    X += rng.uniform(0, 1, X.shape) ** 6 * 0.5
+    Y = M.mole_to_mass(mech, X / X.sum(axis=1, keepdims=True))
+    T = rng.uniform(700, 1500, n)
+    f = W._finish(mech, Y, T, 1e-6, (n,), "c12")
+    g = run_gpu("synth_c12_53", f, kernel="rounds")
+    orc = orc_cache("synth_c12_53")
+    o = orc.react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12, max_order=5)
+    assert (g["status"] == 0).all() and o["nfail"] == 0
+    assert (np.abs(g["T"] - o["T"]) / o["T"]).max() <= T_RTOL
+    tight = orc.react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-12, atol=1e-20, max_order=5)
+    rho = f.rhoY.sum(axis=0)
+    eg = np.abs(g["rhoY"] - tight["rhoY"]).max(axis=0) / rho
+    eo = np.abs(o["rhoY"] - tight["rhoY"]).max(axis=0) / rho
+    assert eg.max() <= 3.0 * eo.max() + 1e-9
+
+
+def test_rounds_forcing_typical_values_and_order(orc_cache):
+    mech = M.builtin("synth_ch4_21")
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 1024, seed=5), dt=1e-5)
+    rng = np.random.default_rng(3)
+    fY = f.rhoY * rng.normal(0, 30.0, f.rhoY.shape)
+    fH = rng.normal(0, 1e9, f.ncells)
+    typ = np.concatenate([np.maximum(1e-10, f.rhoY.mean(axis=1)), [1500.0]])
+    g = run_gpu("synth_ch4_21", f, rtol=1e-6, atol=1e-5, max_order=4, typ=typ, fY=fY, fH=fH, kernel="rounds")
+    o = orc_cache("synth_ch4_21").react(f.rhoY, fY, f.T, f.rhoH, fH, f.dt, rtol=1e-6, atol=1e-5, typ=typ,
+                                        max_order=4)
+    assert ((g["status"] == 0) & (o["status"] == 0)).all()
+    rho = f.rhoY.sum(axis=0)
+    assert (np.abs(g["T"] - o["T"]) / o["T"]).max() < 1e-4
+    assert (np.abs(g["rhoY"] - o["rhoY"]).max(axis=0) / rho).max() < 1e-5
+    assert np.allclose(g["rhoH"], f.rhoH + f.dt * fH, rtol=1e-15)
+
+
+def test_rounds_status_mask_and_bad_inputs(orc_cache):
+    mech = M.builtin("synth_h2_9")
+    f = W.premixed_h2(mech, edge=4)
+    rY, T = f.rhoY.copy(), f.T.copy()
+    rY[0, 1] = np.nan
+    T[2] = -5.0
+    mask = np.ones(f.ncells, np.int32)
+    mask[3] = 0
+    f2 = W.Field(mech, rY, T, f.rhoH.copy(), f.frhoY, f.frhoH, f.dt, f.shape, f.name)
+    g = run_gpu("synth_h2_9", f2, mask=mask, kernel="rounds")
+    assert list(g["status"][:4]) == [0, -4, -4, 1]
+    assert g["fct"][3] == 0
+    assert np.isnan(g["rhoY"][0, 1])
+    assert g["T"][2] == -5.0 and g["T"][3] == f.T[3]
+    assert g["stats"]["n_failed"] == 2 and g["stats"]["n_masked"] == 1
+    f3 = W.premixed_h2(mech, edge=4, dt=1e-3)
+    g = run_gpu("synth_h2_9", f3, max_steps=3, kernel="rounds")
+    o = _oracle(orc_cache, "synth_h2_9", f3, max_steps=3)
+    assert (g["status"] == -1).any()
+    assert ((g["status"] == -1) == (o["status"] == -1)).mean() > 0.9
