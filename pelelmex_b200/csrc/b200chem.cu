@@ -341,21 +341,11 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   R.P = P;
   R.SL = SL;
   R.S = rounds_carve(h->d_rounds, cap, h->N, lut);
-  // the three slot lists follow the carved arrays (each rounded to 256 B)
-  int* lists = nullptr;
-  {
-    const long long n = h->N + 1;
-    size_t used = 0;
-    auto rnd = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    used += rnd(8ull * (rounds::kRCellD) * cap);
-    used += rnd(8ull * (kZn + 7) * n * cap);
-    used += rnd(4ull * rounds::kRCellI * cap);
-    used += rnd(8ull * n * n * cap);
-    used += rnd((size_t)lut * n * n * cap);
-    lists = reinterpret_cast<int*>(static_cast<unsigned char*>(h->d_rounds) + used);
-    if (used + 12ull * cap > h->rounds_bytes)
-      return set_err(B200CHEM_ECUDA, "round-integrator state layout overflows its buffer");
-  }
+  // the three slot lists follow the cell records
+  const size_t rec_bytes = (size_t)R.S.L.stride * cap;
+  if (rec_bytes + 12ull * cap > h->rounds_bytes)
+    return set_err(B200CHEM_ECUDA, "round-integrator state layout overflows its buffer");
+  int* lists = reinterpret_cast<int*>(static_cast<unsigned char*>(h->d_rounds) + rec_bytes);
   int* listA = lists;
   int* listB = lists + cap;
   int* listS = lists + 2 * cap;

@@ -16,11 +16,13 @@
 //                 Gauss-Jordan inverse of D (I - gamma J) D^-1 (FP32);
 //   ctrl kernel   again for the cells that were set up.
 //
-// Per-cell vectors (Nordsieck array, ewt, acor, ...) and matrices are
-// interleaved by cell ("slot"): element e of cell s at base[e * cap + s], so
-// every access of a warp of consecutive slots is one coalesced transaction.
-// The step-control scalars of a cell are one small record (RCell), loaded at
-// the start of a kernel and stored at its end.
+// Each cell ("slot") owns one contiguous record in device memory: its
+// step-control scalars (RCell), its vectors (Nordsieck array, ewt, acor, ...)
+// and its two matrices (FP64 Jacobian and the scaled inverse of the Newton
+// matrix), both column-major.  A thread streams its own record sequentially,
+// so every 32-byte sector it touches is used whole whatever the order of the
+// cells in the work lists; a warp working on one cell reads a matrix column
+// as one coalesced transaction.
 #pragma once
 #include "bdf_group.cuh"
 
@@ -43,61 +45,77 @@ enum Label : int {
 // What the cell needs next.
 enum Need : int { kNeedRhs = 0, kNeedSetup = 1, kDone = 2 };
 
-// Step-control record of one cell (doubles first, then ints).
-struct RCell {
+// Step-control record of one cell (doubles first, then ints), padded to a
+// multiple of 16 bytes so that it moves as 16-byte vectors.
+struct alignas(16) RCell {
   double tau[kZn + 2], tq[6], l[kZn];
   double h, hprime, hscale, eta, etamax, tn, gamma, gammap, gamrat, crate, acnrm, rl1, saved_tq5, gamma_lu;
   double dt, saved_t, delp, hg, hub, hlb;
   int q, qprime, L, qwait, nstlp, nstlj, jcur, ncf, nef, nflag, convfail, callSetup, jbad, mnewt, attempt;
   int count1, hnewOK, nstloc, qmax, max_steps, setup_conv, label, setup_ier;
   CellCounters cnt;
+  int pad_[2];
 };
-constexpr int kRCellD = 2 * kZn + 2 + 6 + 20;  // doubles of RCell
-constexpr int kRCellI = 23 + 7;                // ints of RCell
-static_assert(sizeof(RCell) == kRCellD * 8 + kRCellI * 4, "RCell must be packed doubles then ints");
+static_assert(sizeof(RCell) % 16 == 0, "RCell moves as 16-byte vectors");
+
+// Byte layout of one cell record for n components and inverse type of
+// lut_bytes: [RCell][vectors (kZn + 7) n doubles][J: n columns of ldj
+// doubles][A: n columns of lda LUT], each part 16-byte aligned, the record
+// padded to 128 bytes.
+struct RLayout {
+  int ldj, lda;          // column strides (elements) of J and A
+  int off_vec, off_j, off_a;
+  long long stride;      // bytes per record
+};
+
+__host__ __device__ inline RLayout rounds_record_layout(int n, int lut_bytes) {
+  RLayout L;
+  L.ldj = (n + 1) & ~1;                                  // 16-byte columns
+  L.lda = (lut_bytes == 4) ? ((n + 3) & ~3) : L.ldj;     // 16-byte columns
+  L.off_vec = (int)sizeof(RCell);
+  L.off_j = L.off_vec + ((8 * (kZn + 7) * n + 15) & ~15);
+  L.off_a = L.off_j + 8 * L.ldj * n;
+  L.stride = ((long long)L.off_a + (long long)lut_bytes * L.lda * n + 127) & ~127LL;
+  return L;
+}
 
 // Device-memory state of one chunk of cells.
 struct RState {
-  double* vec;     // [(kZn + 7) * n][cap]: zn[0..5], ewt, acor, ftemp, fv, F, Dsc, yev
-  double* cd;      // [kRCellD][cap] RCell doubles
-  int* ci;         // [kRCellI][cap] RCell ints
-  double* J;       // [n * n][cap] Jacobian (FP64), row-major per cell
-  void* A;         // [n * n][cap] scaled inverse of the Newton matrix (LUT)
-  long long cap;   // slots of the chunk
+  unsigned char* rec;  // [cap][L.stride]
+  RLayout L;
+  long long cap;       // records of the chunk
 };
 
-// Vectors of one cell.
+// Vectors of one cell (contiguous).
 template <int n>
 struct RVec {
-  double* b;  // vec + slot
-  long long cap;
-  __device__ __forceinline__ double& at(int e) const { return b[(long long)e * cap]; }
-  __device__ __forceinline__ double& zn(int j, int i) const { return at(j * n + i); }
-  __device__ __forceinline__ double& ewt(int i) const { return at((kZn + 0) * n + i); }
-  __device__ __forceinline__ double& acor(int i) const { return at((kZn + 1) * n + i); }
-  __device__ __forceinline__ double& ftemp(int i) const { return at((kZn + 2) * n + i); }
-  __device__ __forceinline__ double& fv(int i) const { return at((kZn + 3) * n + i); }
-  __device__ __forceinline__ double& F(int i) const { return at((kZn + 4) * n + i); }
-  __device__ __forceinline__ double& dsc(int i) const { return at((kZn + 5) * n + i); }
-  __device__ __forceinline__ double& yev(int i) const { return at((kZn + 6) * n + i); }
+  double* b;
+  __device__ __forceinline__ double& zn(int j, int i) const { return b[j * n + i]; }
+  __device__ __forceinline__ double& ewt(int i) const { return b[(kZn + 0) * n + i]; }
+  __device__ __forceinline__ double& acor(int i) const { return b[(kZn + 1) * n + i]; }
+  __device__ __forceinline__ double& ftemp(int i) const { return b[(kZn + 2) * n + i]; }
+  __device__ __forceinline__ double& fv(int i) const { return b[(kZn + 3) * n + i]; }
+  __device__ __forceinline__ double& F(int i) const { return b[(kZn + 4) * n + i]; }
+  __device__ __forceinline__ double& dsc(int i) const { return b[(kZn + 5) * n + i]; }
+  __device__ __forceinline__ double& yev(int i) const { return b[(kZn + 6) * n + i]; }
 };
 
-__device__ __forceinline__ void load_cell(RCell& c, const RState& S, long long slot) {
-  double* d = reinterpret_cast<double*>(&c);
-  int* iv = reinterpret_cast<int*>(d + kRCellD);
-#pragma unroll
-  for (int f = 0; f < kRCellD; ++f) d[f] = S.cd[(long long)f * S.cap + slot];
-#pragma unroll
-  for (int f = 0; f < kRCellI; ++f) iv[f] = S.ci[(long long)f * S.cap + slot];
+__device__ __forceinline__ unsigned char* rec_of(const RState& S, long long slot) {
+  return S.rec + slot * S.L.stride;
 }
 
-__device__ __forceinline__ void store_cell(const RCell& c, const RState& S, long long slot) {
-  const double* d = reinterpret_cast<const double*>(&c);
-  const int* iv = reinterpret_cast<const int*>(d + kRCellD);
+__device__ __forceinline__ void load_cell(RCell& c, const unsigned char* rec) {
+  const uint4* src = reinterpret_cast<const uint4*>(rec);
+  uint4* dst = reinterpret_cast<uint4*>(&c);
 #pragma unroll
-  for (int f = 0; f < kRCellD; ++f) S.cd[(long long)f * S.cap + slot] = d[f];
+  for (int k = 0; k < (int)(sizeof(RCell) / 16); ++k) dst[k] = src[k];
+}
+
+__device__ __forceinline__ void store_cell(const RCell& c, unsigned char* rec) {
+  const uint4* src = reinterpret_cast<const uint4*>(&c);
+  uint4* dst = reinterpret_cast<uint4*>(rec);
 #pragma unroll
-  for (int f = 0; f < kRCellI; ++f) S.ci[(long long)f * S.cap + slot] = iv[f];
+  for (int k = 0; k < (int)(sizeof(RCell) / 16); ++k) dst[k] = src[k];
 }
 
 // ---------------------------------------------------------- BDF helpers
@@ -316,21 +334,23 @@ __device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, doubl
   }
 }
 
-// x := D^-1 A D x with the scaled inverse A (interleaved, element (i,j) at
-// A[(i n + j) cap]); LUT = double: A is the plain inverse (no scaling).
+// x := D^-1 A D x with the scaled inverse A (column-major, column stride
+// lda); LUT = double: A is the plain inverse (no scaling).
 template <int n, typename LUT>
-__device__ __forceinline__ void r_apply_inverse(const LUT* A, long long cap, const RVec<n>& v, double (&x)[n]) {
+__device__ __forceinline__ void r_apply_inverse(const LUT* A, int lda, const RVec<n>& v, double (&x)[n]) {
   constexpr bool kScaled = sizeof(LUT) == 4;
-  LUT b[n];
+  LUT acc[n];
 #pragma unroll
-  for (int j = 0; j < n; ++j) b[j] = (LUT)(kScaled ? x[j] * v.dsc(j) : x[j]);
+  for (int i = 0; i < n; ++i) acc[i] = (LUT)0;
 #pragma unroll 1
-  for (int i = 0; i < n; ++i) {
-    LUT acc = (LUT)0;
+  for (int j = 0; j < n; ++j) {
+    const LUT bj = (LUT)(kScaled ? x[j] * v.dsc(j) : x[j]);
+    const LUT* col = A + j * lda;
 #pragma unroll
-    for (int j = 0; j < n; ++j) acc += A[(long long)(i * n + j) * cap] * b[j];
-    x[i] = kScaled ? (double)acc / v.dsc(i) : (double)acc;
+    for (int i = 0; i < n; ++i) acc[i] += col[i] * bj;
   }
+#pragma unroll
+  for (int i = 0; i < n; ++i) x[i] = kScaled ? (double)acc[i] / v.dsc(i) : (double)acc[i];
 }
 
 // Advance the cell from resume point `lab` until it needs a right-hand side
@@ -338,7 +358,7 @@ __device__ __forceinline__ void r_apply_inverse(const LUT* A, long long cap, con
 // a setup (kNeedSetup), or is finished (kDone, *status set).
 template <int n, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
-                                         const double* J, const LUT* A, long long cap, int* status) {
+                                         const double* J, int ldj, const LUT* A, int lda, int* status) {
   for (int guard = 0; guard < 256; ++guard) {
     switch (lab) {
       case kLAfterF0: {
@@ -492,17 +512,22 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
           x[i] = dl[i];
         }
         // solve (I - gamma_lu J) x = dl: FP32 inverse + one FP64 refinement step
-        r_apply_inverse<n, LUT>(A, cap, v, x);
+        r_apply_inverse<n, LUT>(A, lda, v, x);
         if (sizeof(LUT) == 4) {
+          // r = dl - (x - gamma_lu J x), J column-major
           double r[n];
-#pragma unroll 1
-          for (int i = 0; i < n; ++i) {
-            double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < n; ++j) s += J[(long long)(i * n + j) * cap] * x[j];
-            r[i] = dl[i] - (x[i] - c.gamma_lu * s);
+          for (int i = 0; i < n; ++i) r[i] = 0.0;
+#pragma unroll 1
+          for (int j = 0; j < n; ++j) {
+            const double xj = x[j];
+            const double* col = J + j * ldj;
+#pragma unroll
+            for (int i = 0; i < n; ++i) r[i] += col[i] * xj;
           }
-          r_apply_inverse<n, LUT>(A, cap, v, r);
+#pragma unroll
+          for (int i = 0; i < n; ++i) r[i] = dl[i] - (x[i] - c.gamma_lu * r[i]);
+          r_apply_inverse<n, LUT>(A, lda, v, r);
 #pragma unroll
           for (int i = 0; i < n; ++i) x[i] += r[i];
         }

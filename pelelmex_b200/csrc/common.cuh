@@ -114,10 +114,9 @@ enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsSetup };
 
 // Per-warp scratch of the setup kernel.  Shared: C, g/RT, h/RT, Dsc [Npad]
 // (double), rates [Rpad] (double), inverse [n][ldl] + pivot column [Npad]
-// (LUT), pivots [n] (int).  Global: column-major Jacobian [n][ldj] and four
-// per-reaction arrays [Rpad] (double).
+// (LUT), pivots [n] (int).  Global: four per-reaction arrays [Rpad] (double).
 struct RoundsSetupLayout {
-  int Npad, Rpad, ldj, ldl;
+  int Npad, Rpad, ldl;
   int smem_per_warp;
   long long gbytes_per_warp;
 };

@@ -222,7 +222,8 @@ __global__ void __launch_bounds__(128) rk_start(RoundsParams R) {
         code = B200CHEM_CELL_MASKED;
         if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = 0.0;
       } else {
-        const RVec<n> v{R.S.vec + slot, R.S.cap};
+        unsigned char* rec = rec_of(R.S, slot);
+        const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
         const double* yp = elem(bx.rhoY, L.i, L.j, L.k);
         const double* fp = elem(bx.fY, L.i, L.j, L.k);
         double rho = 0.0;
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(128) rk_start(RoundsParams R) {
         } else {
           RCell c;
           r_begin<n>(c, v, P.atol, P.rtol, P.dt, P.qmax, P.max_steps);
-          store_cell(c, R.S, slot);
+          store_cell(c, rec);
           go = true;
         }
       }
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
   double* sW = sG + NS * blockDim.x;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
     const int slot = R.list_in[idx];
-    const RVec<n> v{R.S.vec + slot, R.S.cap};
+    const RVec<n> v{reinterpret_cast<double*>(rec_of(R.S, slot) + R.S.L.off_vec)};
     r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
   }
 }
@@ -282,7 +283,6 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
   constexpr int n = NS + 1;
   const ReactParams& P = R.P;
   const int cnt = *R.cnt_in;
-  const LUT* Abase = reinterpret_cast<const LUT*>(R.S.A);
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < cnt; base += stride) {
     const int idx = base + threadIdx.x;
@@ -291,11 +291,13 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
     RCell c;
     if (live) {
       slot = R.list_in[idx];
-      load_cell(c, R.S, slot);
+      unsigned char* rec = rec_of(R.S, slot);
+      load_cell(c, rec);
       if (after_rhs) c.cnt.nfe++;
-      const RVec<n> v{R.S.vec + slot, R.S.cap};
-      need = r_advance<n, LUT>(c, v, c.label, P.atol, P.rtol, R.S.J + slot, Abase + slot, R.S.cap, &status);
-      store_cell(c, R.S, slot);
+      const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
+      need = r_advance<n, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
+                               R.S.L.ldj, reinterpret_cast<const LUT*>(rec + R.S.L.off_a), R.S.L.lda, &status);
+      store_cell(c, rec);
       if (need == kDone) {
         const long long cell = R.chunk0 + slot;
         const CellLoc L = locate(P, cell);
@@ -347,22 +349,23 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
   LUT* A = reinterpret_cast<LUT*>(ms.q + SL.Rpad);
   LUT* fcol = A + (size_t)n * SL.ldl;
   int* ipiv = reinterpret_cast<int*>(fcol + SL.Npad);
-  // per-warp global scratch: column-major Jacobian and per-reaction terms
+  // per-warp global scratch: per-reaction Jacobian terms
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
-  double* Jw = reinterpret_cast<double*>(R.wscratch + gw * SL.gbytes_per_warp);
-  ms.r1 = Jw + (size_t)n * SL.ldj;
+  ms.r1 = reinterpret_cast<double*>(R.wscratch + gw * SL.gbytes_per_warp);
   ms.r2 = ms.r1 + SL.Rpad;
   ms.r3 = ms.r2 + SL.Rpad;
   ms.r4 = ms.r3 + SL.Rpad;
   const int cnt = *R.cnt_in;
-  const long long cap = R.S.cap;
-  LUT* Ag = reinterpret_cast<LUT*>(R.S.A);
+  const RLayout RL = R.S.L;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long idx = gw; idx < cnt; idx += nwarps) {
     const int slot = R.list_in[idx];
-    const RVec<n> v{R.S.vec + slot, cap};
+    unsigned char* rec = rec_of(R.S, slot);
+    const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
+    double* J = reinterpret_cast<double*>(rec + RL.off_j);  // column-major, kept for refinement
+    LUT* Ar = reinterpret_cast<LUT*>(rec + RL.off_a);
     RCell c;
-    load_cell(c, R.S, slot);
+    load_cell(c, rec);
     const double dgamma = fabs(c.gamma / c.gammap - 1.0);
     const bool jbad = (c.cnt.nst == 0) || (c.cnt.nst >= c.nstlj + kMSBJ) ||
                       (c.setup_conv == kFailBadJ && dgamma < kDGMAX_JBAD) || (c.setup_conv == kFailOther);
@@ -374,25 +377,11 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
         y.v[cc] = (i < n) ? v.yev(i) : 0.0;
         fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
       }
-      grp_jac<32, CPL>(&s_mech, ms, y, fy, Jw, SL.ldj, lane);
-      __syncwarp();
-      // keep the Jacobian for the refinement step and later setups
-      for (int l = 0; l < n; ++l)
-#pragma unroll
-        for (int cc = 0; cc < CPL; ++cc) {
-          const int i = lane + 32 * cc;
-          if (i < n) R.S.J[(long long)(i * n + l) * cap + slot] = Jw[l * SL.ldj + i];
-        }
+      grp_jac<32, CPL>(&s_mech, ms, y, fy, J, RL.ldj, lane);
       c.cnt.nje++;
       c.nstlj = c.cnt.nst;
       c.jcur = 1;
     } else {
-      for (int l = 0; l < n; ++l)
-#pragma unroll
-        for (int cc = 0; cc < CPL; ++cc) {
-          const int i = lane + 32 * cc;
-          if (i < n) Jw[l * SL.ldj + i] = R.S.J[(long long)(i * n + l) * cap + slot];
-        }
       c.jcur = 0;
     }
 #pragma unroll
@@ -405,14 +394,15 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
       }
     }
     __syncwarp();
-    const int ier = grp_gj_inverse<32, LUT>(Jw, SL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, c.gamma, lane);
+    const int ier = grp_gj_inverse<32, LUT>(J, RL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, c.gamma, lane);
     __syncwarp();
+    // the inverse, column-major: lanes over rows write a column contiguously
     if (ier == 0)
-      for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
 #pragma unroll
         for (int cc = 0; cc < CPL; ++cc) {
-          const int j = lane + 32 * cc;
-          if (j < n) Ag[(long long)(i * n + j) * cap + slot] = A[i * SL.ldl + j];
+          const int i = lane + 32 * cc;
+          if (i < n) Ar[j * RL.lda + i] = A[i * SL.ldl + j];
         }
     c.cnt.nlu++;
     c.gamma_lu = c.gamma;
@@ -421,7 +411,8 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
     c.crate = 1.0;
     c.nstlp = c.cnt.nst;
     c.setup_ier = ier;
-    if (lane == 0) store_cell(c, R.S, slot);
+    __syncwarp();
+    if (lane == 0) store_cell(c, rec);
     __syncwarp();
   }
 }
@@ -496,36 +487,23 @@ RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
   const int n = N + 1;
   L.Npad = ((n + 31) / 32) * 32;
   L.Rpad = std::max(32, ((R + 31) / 32) * 32);
-  L.ldj = n | 1;
   L.ldl = n | 1;
   long long b = 8LL * (4 * L.Npad + L.Rpad);
   b += (long long)lut_bytes * ((long long)n * L.ldl + L.Npad);
   b += 4LL * n;
   L.smem_per_warp = (int)((b + 15) & ~15LL);
-  L.gbytes_per_warp = (8LL * ((long long)n * L.ldj + 4LL * L.Rpad) + 255) & ~255LL;
+  L.gbytes_per_warp = (8LL * 4LL * L.Rpad + 255) & ~255LL;
   return L;
 }
 
 long long rounds_state_bytes_per_cell(int N, int lut_bytes) {
-  const long long n = N + 1;
-  return 8LL * (kZn + 7) * n + 8LL * kRCellD + 4LL * kRCellI + 8LL * n * n + (long long)lut_bytes * n * n +
-         4LL * 3;  // three slot lists
+  return rounds_record_layout(N + 1, lut_bytes).stride + 4LL * 3;  // record + three slot lists
 }
 
 RState rounds_carve(void* base, long long cap, int N, int lut_bytes) {
-  const long long n = N + 1;
   RState S;
-  unsigned char* p = static_cast<unsigned char*>(base);
-  auto take = [&](long long bytes) {
-    unsigned char* r = p;
-    p += (bytes + 255) & ~255LL;
-    return r;
-  };
-  S.vec = reinterpret_cast<double*>(take(8LL * (kZn + 7) * n * cap));
-  S.cd = reinterpret_cast<double*>(take(8LL * kRCellD * cap));
-  S.ci = reinterpret_cast<int*>(take(4LL * kRCellI * cap));
-  S.J = reinterpret_cast<double*>(take(8LL * n * n * cap));
-  S.A = take((long long)lut_bytes * n * n * cap);
+  S.rec = static_cast<unsigned char*>(base);
+  S.L = rounds_record_layout(N + 1, lut_bytes);
   S.cap = cap;
   return S;
 }
