@@ -314,8 +314,9 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     return set_err(B200CHEM_EINVAL, "round-based integrator not compiled for N=%d", h->N);
   const int lut = h->opts.lu_fp64 ? 8 : 4;
   const RoundsSetupLayout SL = rounds_setup_layout(h->N, h->R, lut);
-  if (4 * SL.smem_per_warp > h->smem_optin - 2048)
-    return set_err(B200CHEM_ETOOBIG, "setup kernel needs %d B of shared memory per CTA", 4 * SL.smem_per_warp);
+  if (4 * std::max(SL.jac_smem_per_warp, SL.gj_smem_per_warp) > h->smem_optin - 2048)
+    return set_err(B200CHEM_ETOOBIG, "setup kernels need %d B of shared memory per CTA",
+                   4 * std::max(SL.jac_smem_per_warp, SL.gj_smem_per_warp));
   if (h->rgrid_lut != lut) {
     CK(rounds_grids_for(h->N, lut, SL, h->sm_count, &h->rgrid));
     h->rgrid_lut = lut;
@@ -330,7 +331,7 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   const size_t state_bytes = (size_t)per_cell * cap + 16 * 256;
   int err = ensure_buffer(&h->d_rounds, &h->rounds_bytes, state_bytes, st, "round-integrator state");
   if (err) return err;
-  err = ensure_buffer(&h->d_rwarp, &h->rwarp_bytes, (size_t)h->rgrid.setup * 4 * SL.gbytes_per_warp, st,
+  err = ensure_buffer(&h->d_rwarp, &h->rwarp_bytes, (size_t)h->rgrid.jac * 4 * SL.gbytes_per_warp, st,
                       "setup scratch");
   if (err) return err;
   if (!h->d_rcnt) {
@@ -382,7 +383,8 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
       CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 1, st));
       R.list_in = listS;
       R.cnt_in = cntS;
-      CK(rounds_launch(h->N, lut, kRoundsSetup, R, h->rgrid, 0, st));
+      CK(rounds_launch(h->N, lut, kRoundsJac, R, h->rgrid, 0, st));
+      CK(rounds_launch(h->N, lut, kRoundsGj, R, h->rgrid, 0, st));
       // cells coming back from a setup always ask for a right-hand side next
       CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 0, st));
       cur = 1 - cur;

@@ -334,23 +334,145 @@ __device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, doubl
   }
 }
 
-// x := D^-1 A D x with the scaled inverse A (column-major, column stride
-// lda); LUT = double: A is the plain inverse (no scaling).
+// 16-byte vector loads / stores of an n-vector (n even, p 16-byte aligned).
+template <int n>
+__device__ __forceinline__ void vld(const double* p, double (&r)[n]) {
+  static_assert(n % 2 == 0, "records hold even-length vectors");
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int i = 0; i < n / 2; ++i) {
+    const double2 t = q[i];
+    r[2 * i] = t.x;
+    r[2 * i + 1] = t.y;
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void vst(double* p, const double (&r)[n]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int i = 0; i < n / 2; ++i) q[i] = make_double2(r[2 * i], r[2 * i + 1]);
+}
+
+// Column stride of the inverse for n components (the record layout's lda).
 template <int n, typename LUT>
-__device__ __forceinline__ void r_apply_inverse(const LUT* A, int lda, const RVec<n>& v, double (&x)[n]) {
+constexpr int inv_ld() {
+  return sizeof(LUT) == 4 ? (n + 3) / 4 * 4 : (n + 1) / 2 * 2;
+}
+
+// out := D^-1 A D src with the scaled inverse A (column-major, 16-byte
+// columns of inv_ld<n, LUT>() elements) and D = dsc; LUT = double: A is the
+// plain inverse.  src and dsc live in the cell record (L1-resident): the
+// column loop stays rolled, so only the accumulators occupy registers.
+template <int n, typename LUT>
+__device__ __forceinline__ void r_apply_inverse(const LUT* A, const double* dsc, const double* src,
+                                                double (&out)[n]) {
   constexpr bool kScaled = sizeof(LUT) == 4;
-  LUT acc[n];
+  constexpr int V = 16 / (int)sizeof(LUT);
+  constexpr int LD = inv_ld<n, LUT>();
+  LUT acc[LD];
 #pragma unroll
-  for (int i = 0; i < n; ++i) acc[i] = (LUT)0;
-#pragma unroll 1
+  for (int i = 0; i < LD; ++i) acc[i] = (LUT)0;
+#pragma unroll 2
   for (int j = 0; j < n; ++j) {
-    const LUT bj = (LUT)(kScaled ? x[j] * v.dsc(j) : x[j]);
-    const LUT* col = A + j * lda;
+    const LUT bj = (LUT)(kScaled ? src[j] * dsc[j] : src[j]);
+    const uint4* col = reinterpret_cast<const uint4*>(A + j * LD);
 #pragma unroll
-    for (int i = 0; i < n; ++i) acc[i] += col[i] * bj;
+    for (int t = 0; t < LD / V; ++t) {
+      const uint4 u = col[t];
+      if constexpr (sizeof(LUT) == 4) {
+        acc[t * V + 0] += __uint_as_float(u.x) * bj;
+        acc[t * V + 1] += __uint_as_float(u.y) * bj;
+        acc[t * V + 2] += __uint_as_float(u.z) * bj;
+        acc[t * V + 3] += __uint_as_float(u.w) * bj;
+      } else {
+        acc[t * V + 0] += __hiloint2double((int)u.y, (int)u.x) * bj;
+        acc[t * V + 1] += __hiloint2double((int)u.w, (int)u.z) * bj;
+      }
+    }
   }
 #pragma unroll
-  for (int i = 0; i < n; ++i) x[i] = kScaled ? (double)acc[i] / v.dsc(i) : (double)acc[i];
+  for (int i = 0; i < n; ++i) out[i] = kScaled ? (double)acc[i] / dsc[i] : (double)acc[i];
+}
+
+// One Newton correction: x = (I - gamma_lu J)^-1 dl with
+// dl = -(rl1 zn[1] + acor - gamma ftemp) (FP32 inverse + one FP64 refinement
+// step r = dl - (x - gamma_lu J x), x += A r; FP64 inverse: no refinement),
+// scaled by 2 / (1 + gamrat) when gamma has moved since the setup; then
+// acor += x.  Returns the WRMS norms of x (*del) and of the new acor (*anrm).
+// The record's yev and fv vectors (free during the solve: the next
+// evaluation point is written afterwards, f was copied to ftemp) hold the
+// vectors that are multiplied.
+template <int n, typename LUT>
+__device__ __noinline__ void r_newton(double* vb, const double* J, const LUT* A, double rl1, double gamma,
+                                      double gamma_lu, double gamrat, double* del, double* anrm) {
+  static_assert(n % 2 == 0, "records hold even-length vectors");
+  const RVec<n> v{vb};
+  const double* dsc = &v.dsc(0);
+  double* dlv = &v.yev(0);
+  double* xv = &v.fv(0);
+  {
+    const double2* z1 = reinterpret_cast<const double2*>(&v.zn(1, 0));
+    const double2* ac = reinterpret_cast<const double2*>(&v.acor(0));
+    const double2* ft = reinterpret_cast<const double2*>(&v.ftemp(0));
+    double2* o = reinterpret_cast<double2*>(dlv);
+#pragma unroll
+    for (int i = 0; i < n / 2; ++i) {
+      const double2 a = z1[i], b = ac[i], c = ft[i];
+      o[i] = make_double2(-(rl1 * a.x + b.x - gamma * c.x), -(rl1 * a.y + b.y - gamma * c.y));
+    }
+  }
+  double x[n];
+  r_apply_inverse<n, LUT>(A, dsc, dlv, x);
+  if constexpr (sizeof(LUT) == 4) {
+    vst<n>(xv, x);
+    double r[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i) r[i] = 0.0;
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+      const double xj = xv[j];
+      const double2* col = reinterpret_cast<const double2*>(J + j * n);
+#pragma unroll
+      for (int q = 0; q < n / 2; ++q) {
+        const double2 e = col[q];
+        r[2 * q] += e.x * xj;
+        r[2 * q + 1] += e.y * xj;
+      }
+    }
+    const double2* dl2 = reinterpret_cast<const double2*>(dlv);
+#pragma unroll
+    for (int i = 0; i < n / 2; ++i) {
+      const double2 d = dl2[i];
+      r[2 * i] = d.x - (x[2 * i] - gamma_lu * r[2 * i]);
+      r[2 * i + 1] = d.y - (x[2 * i + 1] - gamma_lu * r[2 * i + 1]);
+    }
+    vst<n>(dlv, r);
+    r_apply_inverse<n, LUT>(A, dsc, dlv, r);
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i] += r[i];
+  }
+  if (gamrat != 1.0) {
+    const double sc = 2.0 / (1.0 + gamrat);
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i] *= sc;
+  }
+  double2* ac = reinterpret_cast<double2*>(&v.acor(0));
+  const double2* ew = reinterpret_cast<const double2*>(&v.ewt(0));
+  double s2 = 0.0, a2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < n / 2; ++i) {
+    double2 a = ac[i];
+    const double2 w = ew[i];
+    a.x += x[2 * i];
+    a.y += x[2 * i + 1];
+    ac[i] = a;
+    const double x0 = x[2 * i] * w.x, x1 = x[2 * i + 1] * w.y, a0 = a.x * w.x, a1 = a.y * w.y;
+    s2 += x0 * x0 + x1 * x1;
+    a2 += a0 * a0 + a1 * a1;
+  }
+  *del = sqrt(s2 / n);
+  *anrm = sqrt(a2 / n);
 }
 
 // Advance the cell from resume point `lab` until it needs a right-hand side
@@ -358,7 +480,7 @@ __device__ __forceinline__ void r_apply_inverse(const LUT* A, int lda, const RVe
 // a setup (kNeedSetup), or is finished (kDone, *status set).
 template <int n, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
-                                         const double* J, int ldj, const LUT* A, int lda, int* status) {
+                                         const double* J, const LUT* A, int* status) {
   for (int guard = 0; guard < 256; ++guard) {
     switch (lab) {
       case kLAfterF0: {
@@ -505,51 +627,12 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       }
       case kLNewtonIter: {
         c.cnt.nni++;
-        double dl[n], x[n];
-#pragma unroll
-        for (int i = 0; i < n; ++i) {
-          dl[i] = -(c.rl1 * v.zn(1, i) + v.acor(i) - c.gamma * v.ftemp(i));
-          x[i] = dl[i];
-        }
-        // solve (I - gamma_lu J) x = dl: FP32 inverse + one FP64 refinement step
-        r_apply_inverse<n, LUT>(A, lda, v, x);
-        if (sizeof(LUT) == 4) {
-          // r = dl - (x - gamma_lu J x), J column-major
-          double r[n];
-#pragma unroll
-          for (int i = 0; i < n; ++i) r[i] = 0.0;
-#pragma unroll 1
-          for (int j = 0; j < n; ++j) {
-            const double xj = x[j];
-            const double* col = J + j * ldj;
-#pragma unroll
-            for (int i = 0; i < n; ++i) r[i] += col[i] * xj;
-          }
-#pragma unroll
-          for (int i = 0; i < n; ++i) r[i] = dl[i] - (x[i] - c.gamma_lu * r[i]);
-          r_apply_inverse<n, LUT>(A, lda, v, r);
-#pragma unroll
-          for (int i = 0; i < n; ++i) x[i] += r[i];
-        }
-        if (c.gamrat != 1.0) {
-          const double sc = 2.0 / (1.0 + c.gamrat);
-#pragma unroll
-          for (int i = 0; i < n; ++i) x[i] *= sc;
-        }
-        double s2 = 0.0, a2 = 0.0;
-#pragma unroll
-        for (int i = 0; i < n; ++i) {
-          const double ac = v.acor(i) + x[i];
-          v.acor(i) = ac;
-          const double w = v.ewt(i);
-          s2 += (x[i] * w) * (x[i] * w);
-          a2 += (ac * w) * (ac * w);
-        }
-        const double del = sqrt(s2 / n);
+        double del, anrm;
+        r_newton<n, LUT>(v.b, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, &del, &anrm);
         if (c.mnewt > 0) c.crate = fmax(kCRDOWN * c.crate, del / c.delp);
         const double dcon = del * fmin(1.0, c.crate) / c.tq[4];
         if (dcon <= 1.0) {
-          c.acnrm = (c.mnewt == 0) ? del : sqrt(a2 / n);
+          c.acnrm = (c.mnewt == 0) ? del : anrm;
           c.jcur = 0;
           lab = kLNlsSuccess;
           break;

@@ -110,14 +110,15 @@ cudaError_t tpc_launch(int N, int lut_bytes, const ReactParams& P, const TpcPara
 
 // ------------------------------------------------------ round-based path
 constexpr int kRoundsRhsBlock = 64;  // threads per CTA of the rhs kernel
-enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsSetup };
+enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsJac, kRoundsGj };
 
-// Per-warp scratch of the setup kernel.  Shared: C, g/RT, h/RT, Dsc [Npad]
-// (double), rates [Rpad] (double), inverse [n][ldl] + pivot column [Npad]
-// (LUT), pivots [n] (int).  Global: four per-reaction arrays [Rpad] (double).
+// Per-warp scratch of the setup kernels.  Jacobian kernel, shared: C, g/RT,
+// h/RT [Npad], rates [Rpad] (double); global: four per-reaction arrays [Rpad]
+// (double).  Inverse kernel, shared: Dsc [Npad] (double), matrix [n][ldl] and
+// pivot column [Npad] (LUT), two index arrays [Npad] (int).
 struct RoundsSetupLayout {
   int Npad, Rpad, ldl;
-  int smem_per_warp;
+  int jac_smem_per_warp, gj_smem_per_warp;
   long long gbytes_per_warp;
 };
 
@@ -137,7 +138,7 @@ struct RoundsParams {
 };
 
 struct RoundsGrids {
-  int start, rhs, ctrl, setup;
+  int start, rhs, ctrl, jac, gj;
 };
 
 bool rounds_supported(int N);

@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
       if (after_rhs) c.cnt.nfe++;
       const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
       need = r_advance<n, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
-                               R.S.L.ldj, reinterpret_cast<const LUT*>(rec + R.S.L.off_a), R.S.L.lda, &status);
+                               reinterpret_cast<const LUT*>(rec + R.S.L.off_a), &status);
       store_cell(c, rec);
       if (need == kDone) {
         const long long cell = R.chunk0 + slot;
@@ -326,10 +326,85 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
   }
 }
 
-// Newton-matrix setup, one warp per cell: maybe a fresh analytic Jacobian
-// (CVODE's jbad rule), then the Gauss-Jordan inverse of D (I - gamma J) D^-1.
-template <int NS, typename LUT, int CPL>
-__global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
+// In-place Gauss-Jordan inverse of the scaled Newton matrix D (I - gamma J)
+// D^-1 (FP32, D = diag(dsc)) or I - gamma J (FP64) with partial pivoting, one
+// warp per cell, lane i holding row i in registers (n <= 32).  Rows are never
+// exchanged: step k takes as pivot the unused row p_k with the largest
+// |a[., k]|, and at the end the inverse is (A^-1)[k][j] = X[p_k][q_j] with
+// q_j the step at which row j was the pivot; that permutation is applied
+// while the result is written column-major to Ar.  Xs, prow, pinv: per-warp
+// shared scratch.  Returns 0, or k+1 when no usable pivot is left at step k.
+template <int n, typename LUT>
+__device__ __forceinline__ int reg_gj_inverse(const double* J, int ldj, const double* dsc, double gamma, LUT* Xs,
+                                              int ldl, int* prow, int* pinv, LUT* Ar, int lda, int lane) {
+  static_assert(n <= 32, "one row per lane");
+  constexpr bool kScaled = sizeof(LUT) == 4;
+  const bool row = lane < n;
+  const double di = row ? dsc[lane] : 1.0;
+  const double rdi = 1.0 / di;
+  LUT a[n];
+#pragma unroll
+  for (int j = 0; j < n; ++j) {
+    const double rdj = __shfl_sync(kFull, rdi, j);
+    const double mij = ((lane == j) ? 1.0 : 0.0) - gamma * (row ? J[j * ldj + lane] : 0.0);
+    a[j] = row ? (LUT)(kScaled ? mij * di * rdj : mij) : (LUT)0;
+  }
+  unsigned used = 0;
+  int mystep = -1;
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    LUT best = (row && !((used >> lane) & 1u)) ? fabs(a[k]) : (LUT)-1;
+    int bi = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const LUT ov = __shfl_xor_sync(kFull, best, o);
+      const int oi = __shfl_xor_sync(kFull, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (!(best > (LUT)0)) return k + 1;  // zero or NaN pivot: singular (warp-uniform)
+    const int p = bi;
+    used |= 1u << p;
+    if (lane == p) mystep = k;
+    const LUT inv = (LUT)1 / __shfl_sync(kFull, a[k], p);
+    const LUT f = a[k];
+    if (lane == p) {
+      a[k] = (LUT)1;
+#pragma unroll
+      for (int j = 0; j < n; ++j) a[j] *= inv;
+    } else {
+      a[k] = (LUT)0;
+    }
+#pragma unroll
+    for (int j = 0; j < n; ++j) {
+      const LUT pj = __shfl_sync(kFull, a[j], p);
+      if (lane != p) a[j] -= f * pj;
+    }
+  }
+  if (row) {
+#pragma unroll
+    for (int j = 0; j < n; ++j) Xs[lane * ldl + j] = a[j];
+    pinv[lane] = mystep;
+    prow[mystep] = lane;
+  }
+  __syncwarp();
+  if (lane < n) {
+    const int pk = prow[lane];
+    for (int j = 0; j < n; ++j) Ar[j * lda + lane] = Xs[pk * ldl + pinv[j]];
+  } else if (lane < lda) {
+    for (int j = 0; j < n; ++j) Ar[j * lda + lane] = (LUT)0;  // column padding
+  }
+  __syncwarp();
+  return 0;
+}
+
+// Jacobian refresh for the cells of the setup list whose matrix CVODE's
+// jbad rule marks stale: the analytic FP64 Jacobian (column-major) into the
+// cell record, one warp per cell.
+template <int NS, int CPL>
+__global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
   constexpr int n = NS + 1;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ DevMech s_mech;
@@ -337,19 +412,12 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const RoundsSetupLayout& SL = R.SL;
-  // per-warp shared scratch
-  unsigned char* sb = dsm + (size_t)w * SL.smem_per_warp;
-  double* d = reinterpret_cast<double*>(sb);
+  double* d = reinterpret_cast<double*>(dsm + (size_t)w * SL.jac_smem_per_warp);
   GrpScratch ms;
   ms.C = d;
   ms.gRT = d + SL.Npad;
   ms.hRT = d + 2 * SL.Npad;
-  double* Dsc = d + 3 * SL.Npad;
-  ms.q = d + 4 * SL.Npad;
-  LUT* A = reinterpret_cast<LUT*>(ms.q + SL.Rpad);
-  LUT* fcol = A + (size_t)n * SL.ldl;
-  int* ipiv = reinterpret_cast<int*>(fcol + SL.Npad);
-  // per-warp global scratch: per-reaction Jacobian terms
+  ms.q = d + 3 * SL.Npad;
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
   ms.r1 = reinterpret_cast<double*>(R.wscratch + gw * SL.gbytes_per_warp);
   ms.r2 = ms.r1 + SL.Rpad;
@@ -361,15 +429,13 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
   for (long long idx = gw; idx < cnt; idx += nwarps) {
     const int slot = R.list_in[idx];
     unsigned char* rec = rec_of(R.S, slot);
-    const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
-    double* J = reinterpret_cast<double*>(rec + RL.off_j);  // column-major, kept for refinement
-    LUT* Ar = reinterpret_cast<LUT*>(rec + RL.off_a);
-    RCell c;
-    load_cell(c, rec);
-    const double dgamma = fabs(c.gamma / c.gammap - 1.0);
-    const bool jbad = (c.cnt.nst == 0) || (c.cnt.nst >= c.nstlj + kMSBJ) ||
-                      (c.setup_conv == kFailBadJ && dgamma < kDGMAX_JBAD) || (c.setup_conv == kFailOther);
+    RCell* cp = reinterpret_cast<RCell*>(rec);
+    const int nst = cp->cnt.nst, nstlj = cp->nstlj, sconv = cp->setup_conv;
+    const double dgamma = fabs(cp->gamma / cp->gammap - 1.0);
+    const bool jbad = (nst == 0) || (nst >= nstlj + kMSBJ) || (sconv == kFailBadJ && dgamma < kDGMAX_JBAD) ||
+                      (sconv == kFailOther);
     if (jbad) {
+      const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
       Vec<CPL> y, fy;
 #pragma unroll
       for (int cc = 0; cc < CPL; ++cc) {
@@ -377,13 +443,47 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
         y.v[cc] = (i < n) ? v.yev(i) : 0.0;
         fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
       }
-      grp_jac<32, CPL>(&s_mech, ms, y, fy, J, RL.ldj, lane);
-      c.cnt.nje++;
-      c.nstlj = c.cnt.nst;
-      c.jcur = 1;
-    } else {
-      c.jcur = 0;
+      grp_jac<32, CPL>(&s_mech, ms, y, fy, reinterpret_cast<double*>(rec + RL.off_j), RL.ldj, lane);
+      __syncwarp();
+      if (lane == 0) {
+        cp->cnt.nje++;
+        cp->nstlj = nst;
+        cp->jcur = 1;
+      }
+    } else if (lane == 0) {
+      cp->jcur = 0;
     }
+    __syncwarp();
+  }
+}
+
+// Newton-matrix inverse of the cells of the setup list, one warp per cell:
+// Gauss-Jordan inverse of D (I - gamma J) D^-1 with D = diag(ewt) (FP32) or
+// of I - gamma J (FP64), written column-major into the cell record.
+template <int NS, typename LUT, int CPL>
+__global__ void __launch_bounds__(128) rk_gj(RoundsParams R) {
+  constexpr int n = NS + 1;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const RoundsSetupLayout& SL = R.SL;
+  unsigned char* sb = dsm + (size_t)w * SL.gj_smem_per_warp;
+  double* Dsc = reinterpret_cast<double*>(sb);
+  LUT* A = reinterpret_cast<LUT*>(Dsc + SL.Npad);
+  LUT* fcol = A + (size_t)n * SL.ldl;
+  int* ipiv = reinterpret_cast<int*>(fcol + SL.Npad);
+  int* ipiv2 = ipiv + SL.Npad;
+  const int cnt = *R.cnt_in;
+  const RLayout RL = R.S.L;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long idx = gw; idx < cnt; idx += nwarps) {
+    const int slot = R.list_in[idx];
+    unsigned char* rec = rec_of(R.S, slot);
+    RCell* cp = reinterpret_cast<RCell*>(rec);
+    const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
+    const double* J = reinterpret_cast<const double*>(rec + RL.off_j);
+    LUT* Ar = reinterpret_cast<LUT*>(rec + RL.off_a);
+    const double gamma = cp->gamma;
 #pragma unroll
     for (int cc = 0; cc < CPL; ++cc) {
       const int i = lane + 32 * cc;
@@ -394,25 +494,31 @@ __global__ void __launch_bounds__(128) rk_setup(RoundsParams R) {
       }
     }
     __syncwarp();
-    const int ier = grp_gj_inverse<32, LUT>(J, RL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, c.gamma, lane);
-    __syncwarp();
-    // the inverse, column-major: lanes over rows write a column contiguously
-    if (ier == 0)
-      for (int j = 0; j < n; ++j)
+    int ier;
+    if constexpr (CPL == 1) {
+      ier = reg_gj_inverse<(CPL == 1 ? n : 1), LUT>(J, RL.ldj, Dsc, gamma, A, SL.ldl, ipiv, ipiv2, Ar, RL.lda,
+                                                    lane);
+    } else {
+      ier = grp_gj_inverse<32, LUT>(J, RL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, gamma, lane);
+      __syncwarp();
+      if (ier == 0)
+        for (int j = 0; j < n; ++j)
 #pragma unroll
-        for (int cc = 0; cc < CPL; ++cc) {
-          const int i = lane + 32 * cc;
-          if (i < n) Ar[j * RL.lda + i] = A[i * SL.ldl + j];
-        }
-    c.cnt.nlu++;
-    c.gamma_lu = c.gamma;
-    c.gamrat = 1.0;
-    c.gammap = c.gamma;
-    c.crate = 1.0;
-    c.nstlp = c.cnt.nst;
-    c.setup_ier = ier;
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int i = lane + 32 * cc;
+            if (i < n) Ar[j * RL.lda + i] = A[i * SL.ldl + j];
+          }
+    }
     __syncwarp();
-    if (lane == 0) store_cell(c, rec);
+    if (lane == 0) {
+      cp->cnt.nlu++;
+      cp->gamma_lu = gamma;
+      cp->gamrat = 1.0;
+      cp->gammap = gamma;
+      cp->crate = 1.0;
+      cp->nstlp = cp->cnt.nst;
+      cp->setup_ier = ier;
+    }
     __syncwarp();
   }
 }
@@ -430,8 +536,10 @@ cudaError_t rounds_setup_attrs(const RoundsSetupLayout& SL) {
   cudaError_t e = cudaFuncSetAttribute(rk_rhs<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        rhs_smem<NS>(kRoundsRhsBlock));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rk_setup<NS, LUT, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              4 * SL.smem_per_warp);
+  e = cudaFuncSetAttribute(rk_jac<NS, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * SL.jac_smem_per_warp);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rk_gj<NS, LUT, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              4 * SL.gj_smem_per_warp);
 }
 
 template <int NS, typename LUT>
@@ -447,10 +555,14 @@ cudaError_t rounds_grids(const RoundsSetupLayout& SL, int sm_count, RoundsGrids*
   G->rhs = std::max(1, b) * sm_count;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_ctrl<NS, LUT>, 128, 0)) != cudaSuccess) return e;
   G->ctrl = std::max(1, b) * sm_count;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_setup<NS, LUT, CPL>, 128, 4 * SL.smem_per_warp)) !=
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_jac<NS, CPL>, 128, 4 * SL.jac_smem_per_warp)) !=
       cudaSuccess)
     return e;
-  G->setup = std::max(1, b) * sm_count;
+  G->jac = std::max(1, b) * sm_count;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_gj<NS, LUT, CPL>, 128, 4 * SL.gj_smem_per_warp)) !=
+      cudaSuccess)
+    return e;
+  G->gj = std::max(1, b) * sm_count;
   G->start = 4 * sm_count;
   return cudaSuccess;
 }
@@ -469,8 +581,11 @@ cudaError_t rounds_launch_t(int what, const RoundsParams& R, const RoundsGrids& 
     case kRoundsCtrl:
       rk_ctrl<NS, LUT><<<G.ctrl, 128, 0, st>>>(R, after_rhs);
       break;
-    case kRoundsSetup:
-      rk_setup<NS, LUT, CPL><<<G.setup, 128, 4 * R.SL.smem_per_warp, st>>>(R);
+    case kRoundsJac:
+      rk_jac<NS, CPL><<<G.jac, 128, 4 * R.SL.jac_smem_per_warp, st>>>(R);
+      break;
+    case kRoundsGj:
+      rk_gj<NS, LUT, CPL><<<G.gj, 128, 4 * R.SL.gj_smem_per_warp, st>>>(R);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -488,10 +603,9 @@ RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
   L.Npad = ((n + 31) / 32) * 32;
   L.Rpad = std::max(32, ((R + 31) / 32) * 32);
   L.ldl = n | 1;
-  long long b = 8LL * (4 * L.Npad + L.Rpad);
-  b += (long long)lut_bytes * ((long long)n * L.ldl + L.Npad);
-  b += 4LL * n;
-  L.smem_per_warp = (int)((b + 15) & ~15LL);
+  L.jac_smem_per_warp = (int)(8LL * (3 * L.Npad + L.Rpad));
+  const long long b = 8LL * L.Npad + (long long)lut_bytes * ((long long)n * L.ldl + L.Npad) + 4LL * 2 * L.Npad;
+  L.gj_smem_per_warp = (int)((b + 15) & ~15LL);
   L.gbytes_per_warp = (8LL * 4LL * L.Rpad + 255) & ~255LL;
   return L;
 }
