@@ -118,13 +118,40 @@ __device__ __forceinline__ void store_cell(const RCell& c, unsigned char* rec) {
   for (int k = 0; k < (int)(sizeof(RCell) / 16); ++k) dst[k] = src[k];
 }
 
+
+// ------------------------------------------------------- lane groups
+// The control kernel runs G lanes per cell (G = 8 or 16): lane gl of a group
+// owns components gl, gl + G, ... of every vector; step-control scalars are
+// computed identically by all lanes of the group.
+template <int n, int G, typename F>
+__device__ __forceinline__ void each(int gl, F f) {
+#pragma unroll
+  for (int cc = 0; cc < (n + G - 1) / G; ++cc) {
+    const int i = gl + G * cc;
+    if (i < n) f(i);
+  }
+}
+
+template <int G>
+__device__ __forceinline__ double gsum(double v, unsigned gm) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, G);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ double gmax(double v, unsigned gm) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(gm, v, o, G));
+  return v;
+}
+
 // ---------------------------------------------------------- BDF helpers
-template <int n>
-__device__ __forceinline__ void r_rescale(RCell& c, const RVec<n>& v) {
+template <int n, int G>
+__device__ __forceinline__ void r_rescale(RCell& c, const RVec<n>& v, int gl) {
   double factor = c.eta;
   for (int j = 1; j <= c.q; ++j) {
-#pragma unroll 4
-    for (int i = 0; i < n; ++i) v.zn(j, i) *= factor;
+    each<n, G>(gl, [&](int i) { v.zn(j, i) *= factor; });
     factor *= c.eta;
   }
   c.h = c.hscale * c.eta;
@@ -132,12 +159,11 @@ __device__ __forceinline__ void r_rescale(RCell& c, const RVec<n>& v) {
 }
 
 // Nordsieck prediction zn := zn * Pascal, column by column in registers.
-template <int n>
-__device__ __forceinline__ void r_predict(RCell& c, const RVec<n>& v) {
+template <int n, int G>
+__device__ __forceinline__ void r_predict(RCell& c, const RVec<n>& v, int gl) {
   c.tn += c.h;
   const int q = c.q;
-#pragma unroll 2
-  for (int i = 0; i < n; ++i) {
+  each<n, G>(gl, [&](int i) {
     double z[kZn];
 #pragma unroll
     for (int j = 0; j < kZn; ++j) z[j] = (j <= q) ? v.zn(j, i) : 0.0;
@@ -149,15 +175,14 @@ __device__ __forceinline__ void r_predict(RCell& c, const RVec<n>& v) {
 #pragma unroll
     for (int j = 0; j < kZn - 1; ++j)
       if (j < q) v.zn(j, i) = z[j];
-  }
+  });
 }
 
-template <int n>
-__device__ __forceinline__ void r_restore(RCell& c, const RVec<n>& v) {
+template <int n, int G>
+__device__ __forceinline__ void r_restore(RCell& c, const RVec<n>& v, int gl) {
   c.tn = c.saved_t;
   const int q = c.q;
-#pragma unroll 2
-  for (int i = 0; i < n; ++i) {
+  each<n, G>(gl, [&](int i) {
     double z[kZn];
 #pragma unroll
     for (int j = 0; j < kZn; ++j) z[j] = (j <= q) ? v.zn(j, i) : 0.0;
@@ -169,22 +194,20 @@ __device__ __forceinline__ void r_restore(RCell& c, const RVec<n>& v) {
 #pragma unroll
     for (int j = 0; j < kZn - 1; ++j)
       if (j < q) v.zn(j, i) = z[j];
-  }
+  });
 }
 
-// WRMS norm of a vector given element-wise by get(i).
-template <int n, typename Get>
-__device__ __forceinline__ double r_wrms(const RVec<n>& v, Get get) {
+// WRMS norm of a vector given element-wise by get(i) (group reduction).
+template <int n, int G, typename Get>
+__device__ __forceinline__ double r_wrms(const RVec<n>& v, int gl, unsigned gm, Get get) {
   double s = 0.0;
-#pragma unroll 4
-  for (int i = 0; i < n; ++i) {
+  each<n, G>(gl, [&](int i) {
     const double t = get(i) * v.ewt(i);
     s += t * t;
-  }
-  return sqrt(s / n);
+  });
+  return sqrt(gsum<G>(s, gm) / n);
 }
 
-template <int n>
 __device__ __forceinline__ void r_set_bdf(RCell& c) {
   const int q = c.q;
   double xi_inv = 1.0, xistar_inv = 1.0;
@@ -233,8 +256,8 @@ __device__ __forceinline__ void r_set_bdf(RCell& c) {
   c.gamrat = (c.cnt.nst > 0) ? c.gamma / c.gammap : 1.0;
 }
 
-template <int n>
-__device__ __forceinline__ void r_increase(RCell& c, const RVec<n>& v) {
+template <int n, int G>
+__device__ __forceinline__ void r_increase(RCell& c, const RVec<n>& v, int gl) {
   const int q = c.q;
   for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
   double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = c.hscale;
@@ -249,16 +272,15 @@ __device__ __forceinline__ void r_increase(RCell& c, const RVec<n>& v) {
     xiold = xi;
   }
   const double A1 = (-alpha0 - alpha1) / prod;
-#pragma unroll 2
-  for (int i = 0; i < n; ++i) {
+  each<n, G>(gl, [&](int i) {
     const double z = A1 * v.zn(c.qmax, i);
     v.zn(q + 1, i) = z;
     for (int j = 2; j <= q; ++j) v.zn(j, i) += c.l[j] * z;
-  }
+  });
 }
 
-template <int n>
-__device__ __forceinline__ void r_decrease(RCell& c, const RVec<n>& v) {
+template <int n, int G>
+__device__ __forceinline__ void r_decrease(RCell& c, const RVec<n>& v, int gl) {
   const int q = c.q;
   for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
   c.l[2] = 1.0;
@@ -268,21 +290,19 @@ __device__ __forceinline__ void r_decrease(RCell& c, const RVec<n>& v) {
     const double xi = hsum / c.hscale;
     for (int i = j + 2; i >= 2; --i) c.l[i] = c.l[i] * xi + c.l[i - 1];
   }
-#pragma unroll 2
-  for (int i = 0; i < n; ++i) {
+  each<n, G>(gl, [&](int i) {
     const double zq = v.zn(q, i);
     for (int j = 2; j < q; ++j) v.zn(j, i) -= c.l[j] * zq;
-  }
+  });
 }
 
-template <int n>
-__device__ __forceinline__ void r_set_ewt(const RVec<n>& v, const double* atolv, double rtol) {
-#pragma unroll 4
-  for (int i = 0; i < n; ++i) v.ewt(i) = 1.0 / (rtol * fabs(v.zn(0, i)) + __ldg(atolv + i));
+template <int n, int G>
+__device__ __forceinline__ void r_set_ewt(const RVec<n>& v, const double* atolv, double rtol, int gl) {
+  each<n, G>(gl, [&](int i) { v.ewt(i) = 1.0 / (rtol * fabs(v.zn(0, i)) + __ldg(atolv + i)); });
 }
 
-template <int n>
-__device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, double dsm) {
+template <int n, int G>
+__device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, double dsm, int gl, unsigned gm) {
   if (c.etamax == 1.0) {
     c.qwait = c.qwait > 2 ? c.qwait : 2;
     c.qprime = c.q;
@@ -299,13 +319,14 @@ __device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, doubl
     double etaqm1 = 0.0, etaqp1 = 0.0;
     if (c.q > 1) {
       const int q = c.q;
-      const double ddn = r_wrms<n>(v, [&](int i) { return v.zn(q, i); }) * c.tq[1];
+      const double ddn = r_wrms<n, G>(v, gl, gm, [&](int i) { return v.zn(q, i); }) * c.tq[1];
       etaqm1 = 1.0 / (pow(kBIAS1 * ddn, 1.0 / c.q) + kADDON);
     }
     if (c.q != c.qmax && c.saved_tq5 != 0.0) {
       const double cquot = (c.tq[5] / c.saved_tq5) * pow(c.h / c.tau[2], (double)c.L);
       const int qm = c.qmax;
-      const double dup = r_wrms<n>(v, [&](int i) { return v.acor(i) - cquot * v.zn(qm, i); }) * c.tq[3];
+      const double dup =
+          r_wrms<n, G>(v, gl, gm, [&](int i) { return v.acor(i) - cquot * v.zn(qm, i); }) * c.tq[3];
       etaqp1 = 1.0 / (pow(kBIAS3 * dup, 1.0 / (c.L + 1)) + kADDON);
     }
     const double etam = fmax(etaqm1, fmax(etaq, etaqp1));
@@ -321,8 +342,8 @@ __device__ __forceinline__ void r_prepare_next(RCell& c, const RVec<n>& v, doubl
     } else {
       c.eta = etaqp1;
       c.qprime = c.q + 1;
-#pragma unroll 4
-      for (int i = 0; i < n; ++i) v.zn(c.qmax, i) = v.acor(i);
+      const int qm = c.qmax;
+      each<n, G>(gl, [&](int i) { v.zn(qm, i) = v.acor(i); });
     }
   }
   if (c.eta < kTHRESH) {
@@ -360,39 +381,35 @@ constexpr int inv_ld() {
   return sizeof(LUT) == 4 ? (n + 3) / 4 * 4 : (n + 1) / 2 * 2;
 }
 
-// out := D^-1 A D src with the scaled inverse A (column-major, 16-byte
-// columns of inv_ld<n, LUT>() elements) and D = dsc; LUT = double: A is the
-// plain inverse.  src and dsc live in the cell record (L1-resident): the
-// column loop stays rolled, so only the accumulators occupy registers.
-template <int n, typename LUT>
-__device__ __forceinline__ void r_apply_inverse(const LUT* A, const double* dsc, const double* src,
-                                                double (&out)[n]) {
+// x := D^-1 A D x for the group's cell: A is the scaled inverse
+// (column-major, 16-byte columns of inv_ld<n, LUT>() elements), D = dsc;
+// LUT = double: A is the plain inverse.  Lane gl holds components gl + G cc
+// of x and dsc; the multiplier of column j comes from its owner lane by
+// shuffle and lanes read consecutive elements of the column.
+template <int n, int G, typename LUT>
+__device__ __forceinline__ void g_apply_inverse(const LUT* A, const double (&dsc)[(n + G - 1) / G],
+                                                double (&x)[(n + G - 1) / G], int gl, unsigned gm) {
+  constexpr int CPL = (n + G - 1) / G;
   constexpr bool kScaled = sizeof(LUT) == 4;
-  constexpr int V = 16 / (int)sizeof(LUT);
   constexpr int LD = inv_ld<n, LUT>();
-  LUT acc[LD];
+  LUT acc[CPL], bs[CPL];
 #pragma unroll
-  for (int i = 0; i < LD; ++i) acc[i] = (LUT)0;
-#pragma unroll 2
+  for (int cc = 0; cc < CPL; ++cc) {
+    acc[cc] = (LUT)0;
+    bs[cc] = (LUT)(kScaled ? x[cc] * dsc[cc] : x[cc]);
+  }
+#pragma unroll
   for (int j = 0; j < n; ++j) {
-    const LUT bj = (LUT)(kScaled ? src[j] * dsc[j] : src[j]);
-    const uint4* col = reinterpret_cast<const uint4*>(A + j * LD);
+    const LUT bj = __shfl_sync(gm, bs[j / G], j % G, G);
+    const LUT* col = A + j * LD;
 #pragma unroll
-    for (int t = 0; t < LD / V; ++t) {
-      const uint4 u = col[t];
-      if constexpr (sizeof(LUT) == 4) {
-        acc[t * V + 0] += __uint_as_float(u.x) * bj;
-        acc[t * V + 1] += __uint_as_float(u.y) * bj;
-        acc[t * V + 2] += __uint_as_float(u.z) * bj;
-        acc[t * V + 3] += __uint_as_float(u.w) * bj;
-      } else {
-        acc[t * V + 0] += __hiloint2double((int)u.y, (int)u.x) * bj;
-        acc[t * V + 1] += __hiloint2double((int)u.w, (int)u.z) * bj;
-      }
+    for (int cc = 0; cc < CPL; ++cc) {
+      const int i = gl + G * cc;
+      if (i < n) acc[cc] += col[i] * bj;
     }
   }
 #pragma unroll
-  for (int i = 0; i < n; ++i) out[i] = kScaled ? (double)acc[i] / dsc[i] : (double)acc[i];
+  for (int cc = 0; cc < CPL; ++cc) x[cc] = kScaled ? (double)acc[cc] / dsc[cc] : (double)acc[cc];
 }
 
 // One Newton correction: x = (I - gamma_lu J)^-1 dl with
@@ -400,99 +417,78 @@ __device__ __forceinline__ void r_apply_inverse(const LUT* A, const double* dsc,
 // step r = dl - (x - gamma_lu J x), x += A r; FP64 inverse: no refinement),
 // scaled by 2 / (1 + gamrat) when gamma has moved since the setup; then
 // acor += x.  Returns the WRMS norms of x (*del) and of the new acor (*anrm).
-// The record's yev and fv vectors (free during the solve: the next
-// evaluation point is written afterwards, f was copied to ftemp) hold the
-// vectors that are multiplied.
-template <int n, typename LUT>
-__device__ __noinline__ void r_newton(double* vb, const double* J, const LUT* A, double rl1, double gamma,
-                                      double gamma_lu, double gamrat, double* del, double* anrm) {
-  static_assert(n % 2 == 0, "records hold even-length vectors");
-  const RVec<n> v{vb};
-  const double* dsc = &v.dsc(0);
-  double* dlv = &v.yev(0);
-  double* xv = &v.fv(0);
-  {
-    const double2* z1 = reinterpret_cast<const double2*>(&v.zn(1, 0));
-    const double2* ac = reinterpret_cast<const double2*>(&v.acor(0));
-    const double2* ft = reinterpret_cast<const double2*>(&v.ftemp(0));
-    double2* o = reinterpret_cast<double2*>(dlv);
+template <int n, int G, typename LUT>
+__device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, const LUT* A, double rl1, double gamma,
+                                         double gamma_lu, double gamrat, int gl, unsigned gm, double* del,
+                                         double* anrm) {
+  constexpr int CPL = (n + G - 1) / G;
+  double dl[CPL], x[CPL], dsc[CPL];
 #pragma unroll
-    for (int i = 0; i < n / 2; ++i) {
-      const double2 a = z1[i], b = ac[i], c = ft[i];
-      o[i] = make_double2(-(rl1 * a.x + b.x - gamma * c.x), -(rl1 * a.y + b.y - gamma * c.y));
-    }
+  for (int cc = 0; cc < CPL; ++cc) {
+    const int i = gl + G * cc;
+    dl[cc] = (i < n) ? -(rl1 * v.zn(1, i) + v.acor(i) - gamma * v.ftemp(i)) : 0.0;
+    dsc[cc] = (i < n) ? v.dsc(i) : 1.0;
+    x[cc] = dl[cc];
   }
-  double x[n];
-  r_apply_inverse<n, LUT>(A, dsc, dlv, x);
+  g_apply_inverse<n, G, LUT>(A, dsc, x, gl, gm);
   if constexpr (sizeof(LUT) == 4) {
-    vst<n>(xv, x);
-    double r[n];
+    constexpr int LDJ = (n + 1) / 2 * 2;
+    double r[CPL];
 #pragma unroll
-    for (int i = 0; i < n; ++i) r[i] = 0.0;
-#pragma unroll 2
+    for (int cc = 0; cc < CPL; ++cc) r[cc] = 0.0;
+#pragma unroll
     for (int j = 0; j < n; ++j) {
-      const double xj = xv[j];
-      const double2* col = reinterpret_cast<const double2*>(J + j * n);
+      const double xj = __shfl_sync(gm, x[j / G], j % G, G);
+      const double* col = J + j * LDJ;
 #pragma unroll
-      for (int q = 0; q < n / 2; ++q) {
-        const double2 e = col[q];
-        r[2 * q] += e.x * xj;
-        r[2 * q + 1] += e.y * xj;
+      for (int cc = 0; cc < CPL; ++cc) {
+        const int i = gl + G * cc;
+        if (i < n) r[cc] += col[i] * xj;
       }
     }
-    const double2* dl2 = reinterpret_cast<const double2*>(dlv);
 #pragma unroll
-    for (int i = 0; i < n / 2; ++i) {
-      const double2 d = dl2[i];
-      r[2 * i] = d.x - (x[2 * i] - gamma_lu * r[2 * i]);
-      r[2 * i + 1] = d.y - (x[2 * i + 1] - gamma_lu * r[2 * i + 1]);
-    }
-    vst<n>(dlv, r);
-    r_apply_inverse<n, LUT>(A, dsc, dlv, r);
+    for (int cc = 0; cc < CPL; ++cc) r[cc] = dl[cc] - (x[cc] - gamma_lu * r[cc]);
+    g_apply_inverse<n, G, LUT>(A, dsc, r, gl, gm);
 #pragma unroll
-    for (int i = 0; i < n; ++i) x[i] += r[i];
+    for (int cc = 0; cc < CPL; ++cc) x[cc] += r[cc];
   }
-  if (gamrat != 1.0) {
-    const double sc = 2.0 / (1.0 + gamrat);
-#pragma unroll
-    for (int i = 0; i < n; ++i) x[i] *= sc;
-  }
-  double2* ac = reinterpret_cast<double2*>(&v.acor(0));
-  const double2* ew = reinterpret_cast<const double2*>(&v.ewt(0));
+  const double sc = (gamrat != 1.0) ? 2.0 / (1.0 + gamrat) : 1.0;
   double s2 = 0.0, a2 = 0.0;
 #pragma unroll
-  for (int i = 0; i < n / 2; ++i) {
-    double2 a = ac[i];
-    const double2 w = ew[i];
-    a.x += x[2 * i];
-    a.y += x[2 * i + 1];
-    ac[i] = a;
-    const double x0 = x[2 * i] * w.x, x1 = x[2 * i + 1] * w.y, a0 = a.x * w.x, a1 = a.y * w.y;
-    s2 += x0 * x0 + x1 * x1;
-    a2 += a0 * a0 + a1 * a1;
+  for (int cc = 0; cc < CPL; ++cc) {
+    const int i = gl + G * cc;
+    if (i < n) {
+      const double xi = x[cc] * sc;
+      const double ac = v.acor(i) + xi;
+      v.acor(i) = ac;
+      const double w = v.ewt(i);
+      s2 += (xi * w) * (xi * w);
+      a2 += (ac * w) * (ac * w);
+    }
   }
-  *del = sqrt(s2 / n);
-  *anrm = sqrt(a2 / n);
+  *del = sqrt(gsum<G>(s2, gm) / n);
+  *anrm = sqrt(gsum<G>(a2, gm) / n);
 }
 
 // Advance the cell from resume point `lab` until it needs a right-hand side
 // at v.yev (returns kNeedRhs with c.label set to the label that consumes it),
 // a setup (kNeedSetup), or is finished (kDone, *status set).
-template <int n, typename LUT>
+template <int n, int G, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
-                                         const double* J, const LUT* A, int* status) {
+                                         const double* J, const LUT* A, int gl, unsigned gm, int* status) {
   for (int guard = 0; guard < 256; ++guard) {
     switch (lab) {
       case kLAfterF0: {
         bool bad = false;
         double hinv = 0.0;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) {
+        each<n, G>(gl, [&](int i) {
           const double f = v.fv(i);
           v.zn(1, i) = f;
           bad |= !isfinite(f);
           hinv = fmax(hinv, fabs(f) / (0.1 * fabs(v.zn(0, i)) + __ldg(atolv + i)));
-        }
+        });
+        hinv = gmax<G>(hinv, gm);
+        bad = gmax<G>(bad ? 1.0 : 0.0, gm) > 0.0;
         if (bad) {
           *status = -4;
           return kDone;
@@ -511,14 +507,16 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         }
         c.count1 = 1;
         c.hnewOK = 0;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + c.hg * v.zn(1, i);
+        {
+          const double hg = c.hg;
+          each<n, G>(gl, [&](int i) { v.yev(i) = v.zn(0, i) + hg * v.zn(1, i); });
+        }
         c.label = kLAfterHin;
         return kNeedRhs;
       }
       case kLAfterHin: {
         const double hg = c.hg;
-        const double yddnrm = r_wrms<n>(v, [&](int i) { return (v.fv(i) - v.zn(1, i)) / hg; });
+        const double yddnrm = r_wrms<n, G>(v, gl, gm, [&](int i) { return (v.fv(i) - v.zn(1, i)) / hg; });
         const double hnew = (yddnrm * c.hub * c.hub > 2.0) ? sqrt(2.0 / yddnrm) : sqrt(c.hg * c.hub);
         bool stop = false;
         if (c.hnewOK) {
@@ -537,8 +535,8 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
           if (c.count1 > 4) stop = true;
         }
         if (!stop) {
-#pragma unroll 4
-          for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + c.hg * v.zn(1, i);
+          const double hg2 = c.hg;
+          each<n, G>(gl, [&](int i) { v.yev(i) = v.zn(0, i) + hg2 * v.zn(1, i); });
           c.label = kLAfterHin;
           return kNeedRhs;
         }
@@ -553,14 +551,13 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       case kLStart: {
         const double h0 = c.h;
         c.hscale = c.hprime = h0;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.zn(1, i) *= h0;
+        each<n, G>(gl, [&](int i) { v.zn(1, i) *= h0; });
         c.nstloc = 0;
         lab = kLBeginStep;
         break;
       }
       case kLBeginStep: {
-        if (c.cnt.nst > 0) r_set_ewt<n>(v, atolv, rtol);
+        if (c.cnt.nst > 0) r_set_ewt<n, G>(v, atolv, rtol, gl);
         if (c.nstloc >= c.max_steps) {
           *status = -1;
           return kDone;
@@ -570,20 +567,20 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         c.nflag = kFirstCall;
         if (c.cnt.nst > 0 && c.hprime != c.h) {
           if (c.qprime != c.q) {
-            if (c.qprime - c.q == 1) r_increase<n>(c, v);
-            else if (c.qprime - c.q == -1) r_decrease<n>(c, v);
+            if (c.qprime - c.q == 1) r_increase<n, G>(c, v, gl);
+            else if (c.qprime - c.q == -1) r_decrease<n, G>(c, v, gl);
             c.q = c.qprime;
             c.L = c.q + 1;
             c.qwait = c.L;
           }
-          r_rescale<n>(c, v);
+          r_rescale<n, G>(c, v, gl);
         }
         lab = kLAttempt;
         break;
       }
       case kLAttempt: {
-        r_predict<n>(c, v);
-        r_set_bdf<n>(c);
+        r_predict<n, G>(c, v, gl);
+        r_set_bdf(c);
         c.convfail = (c.nflag == kFirstCall || c.nflag == kPrevErrFail) ? kNoFailures : kFailOther;
         c.callSetup = (c.nflag == kPrevConvFail) || (c.nflag == kPrevErrFail) || (c.cnt.nst == 0) ||
                       (c.cnt.nst >= c.nstlp + kMSBP) || (fabs(c.gamrat - 1.0) > kDGMAX_LSETUP);
@@ -593,17 +590,15 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         break;
       }
       case kLNlsAttempt: {
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) {
+        each<n, G>(gl, [&](int i) {
           v.acor(i) = 0.0;
           v.yev(i) = v.zn(0, i);
-        }
+        });
         c.label = kLAfterNStart;
         return kNeedRhs;
       }
       case kLAfterNStart: {
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.ftemp(i) = v.fv(i);
+        each<n, G>(gl, [&](int i) { v.ftemp(i) = v.fv(i); });
         if (c.callSetup) {
           c.setup_conv = c.jbad ? kFailBadJ : c.convfail;
           c.label = kLAfterSetup;
@@ -628,7 +623,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       case kLNewtonIter: {
         c.cnt.nni++;
         double del, anrm;
-        r_newton<n, LUT>(v.b, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, &del, &anrm);
+        g_newton<n, G, LUT>(v, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, gl, gm, &del, &anrm);
         if (c.mnewt > 0) c.crate = fmax(kCRDOWN * c.crate, del / c.delp);
         const double dcon = del * fmin(1.0, c.crate) / c.tq[4];
         if (dcon <= 1.0) {
@@ -643,14 +638,12 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         }
         c.delp = del;
         c.mnewt++;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i) + v.acor(i);
+        each<n, G>(gl, [&](int i) { v.yev(i) = v.zn(0, i) + v.acor(i); });
         c.label = kLAfterNIter;
         return kNeedRhs;
       }
       case kLAfterNIter: {
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.ftemp(i) = v.fv(i);
+        each<n, G>(gl, [&](int i) { v.ftemp(i) = v.fv(i); });
         lab = kLNewtonIter;
         break;
       }
@@ -668,7 +661,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       case kLNlsFail1:
       case kLNlsFail2: {
         c.cnt.ncfn++;
-        r_restore<n>(c, v);
+        r_restore<n, G>(c, v, gl);
         c.ncf++;
         c.etamax = 1.0;
         if (c.ncf == kMXNCF) {
@@ -677,7 +670,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         }
         c.eta = kETACF;
         c.nflag = kPrevConvFail;
-        r_rescale<n>(c, v);
+        r_rescale<n, G>(c, v, gl);
         lab = kLAttempt;
         break;
       }
@@ -691,15 +684,15 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
           c.tau[1] = c.h;
           const int q = c.q;
           const bool save = (c.qwait - 1 == 1 && q != c.qmax);
-#pragma unroll 2
-          for (int i = 0; i < n; ++i) {
+          const int qm = c.qmax;
+          each<n, G>(gl, [&](int i) {
             const double ac = v.acor(i);
             for (int j = 0; j <= q; ++j) v.zn(j, i) += c.l[j] * ac;
-            if (save) v.zn(c.qmax, i) = ac;
-          }
+            if (save) v.zn(qm, i) = ac;
+          });
           c.qwait--;
           if (save) c.saved_tq5 = c.tq[5];
-          r_prepare_next<n>(c, v, dsm);
+          r_prepare_next<n, G>(c, v, dsm, gl, gm);
           c.etamax = (c.cnt.nst <= kSMALL_NST) ? kETAMX2 : kETAMX3;
           c.nstloc++;
           if (c.tn - c.dt >= 0.0) {
@@ -712,7 +705,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         c.nef++;
         c.cnt.netf++;
         c.nflag = kPrevErrFail;
-        r_restore<n>(c, v);
+        r_restore<n, G>(c, v, gl);
         if (c.nef == kMXNEF) {
           *status = -2;
           return kDone;
@@ -722,17 +715,17 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
           c.eta = 1.0 / (pow(kBIAS2 * dsm, 1.0 / c.L) + kADDON);
           c.eta = fmax(kETAMIN, c.eta);
           if (c.nef >= kSMALL_NEF) c.eta = fmin(c.eta, kETAMXF);
-          r_rescale<n>(c, v);
+          r_rescale<n, G>(c, v, gl);
           lab = kLAttempt;
           break;
         }
         if (c.q > 1) {
           c.eta = kETAMIN;
-          r_decrease<n>(c, v);
+          r_decrease<n, G>(c, v, gl);
           c.L = c.q;
           c.q--;
           c.qwait = c.L;
-          r_rescale<n>(c, v);
+          r_rescale<n, G>(c, v, gl);
           lab = kLAttempt;
           break;
         }
@@ -740,14 +733,13 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         c.h *= c.eta;
         c.hscale = c.h;
         c.qwait = kLONG_WAIT;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.yev(i) = v.zn(0, i);
+        each<n, G>(gl, [&](int i) { v.yev(i) = v.zn(0, i); });
         c.label = kLAfterRestart;
         return kNeedRhs;
       }
       case kLAfterRestart: {
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) v.zn(1, i) = c.h * v.fv(i);
+        const double hh = c.h;
+        each<n, G>(gl, [&](int i) { v.zn(1, i) = hh * v.fv(i); });
         lab = kLAttempt;
         break;
       }
@@ -764,7 +756,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
 // step-control defaults, then ask for f(y0).
 template <int n>
 __device__ __forceinline__ void r_begin(RCell& c, const RVec<n>& v, const double* atolv, double rtol, double dt,
-                                        int qmax, int max_steps) {
+                                        int qmax, int max_steps) {  // one thread per cell
   c.tn = 0.0;
   c.dt = dt;
   c.cnt = CellCounters{0, 0, 0, 0, 0, 0, 0};
@@ -797,7 +789,7 @@ __device__ __forceinline__ void r_begin(RCell& c, const RVec<n>& v, const double
     v.acor(i) = 0.0;
     v.yev(i) = v.zn(0, i);
   }
-  r_set_ewt<n>(v, atolv, rtol);
+  r_set_ewt<n, 1>(v, atolv, rtol, 0);
   c.label = kLAfterF0;
 }
 

@@ -276,16 +276,25 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
   }
 }
 
-// Resume the cells of list_in.  after_rhs: each consumes the f just
-// evaluated (counted in nfe); otherwise they come back from a setup.
+// Lanes per cell of the control kernel.
+constexpr int ctrl_group(int n) { return n <= 32 ? 8 : 16; }
+
+// Resume the cells of list_in, G lanes per cell.  after_rhs: each consumes
+// the f just evaluated (counted in nfe); otherwise they come back from a
+// setup.
 template <int NS, typename LUT>
 __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
   constexpr int n = NS + 1;
+  constexpr int G = ctrl_group(n);
+  constexpr int GPW = 32 / G;  // cells per warp
   const ReactParams& P = R.P;
   const int cnt = *R.cnt_in;
-  const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < cnt; base += stride) {
-    const int idx = base + threadIdx.x;
+  const int lane = threadIdx.x & 31, gl = lane % G, gi = lane / G;
+  const unsigned gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gi * G));
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int base = wid * GPW; base < cnt; base += nw * GPW) {
+    const int idx = base + gi;
     const bool live = idx < cnt;
     int slot = 0, need = kDone, status = 0;
     RCell c;
@@ -295,9 +304,10 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
       load_cell(c, rec);
       if (after_rhs) c.cnt.nfe++;
       const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
-      need = r_advance<n, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
-                               reinterpret_cast<const LUT*>(rec + R.S.L.off_a), &status);
-      store_cell(c, rec);
+      need = r_advance<n, G, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
+                                  reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status);
+      __syncwarp(gm);
+      if (gl == 0) store_cell(c, rec);
       if (need == kDone) {
         const long long cell = R.chunk0 + slot;
         const CellLoc L = locate(P, cell);
@@ -306,23 +316,28 @@ __global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
           // y(dt) from the Nordsieck array (Horner in s = (dt - tn) / h)
           const double s = (P.dt - c.tn) / c.h;
           double* yp = elem(bx.rhoY, L.i, L.j, L.k);
-#pragma unroll 2
-          for (int q = 0; q < n; ++q) {
-            double y = v.zn(c.q, q);
-            for (int jj = c.q - 1; jj >= 0; --jj) y = v.zn(jj, q) + s * y;
-            if (q < NS) yp[q * bx.rhoY.ns] = y;
+          const int q = c.q;
+          each<n, G>(gl, [&](int k) {
+            double y = v.zn(q, k);
+            for (int jj = q - 1; jj >= 0; --jj) y = v.zn(jj, k) + s * y;
+            if (k < NS) yp[k * bx.rhoY.ns] = y;
             else *elem(bx.T, L.i, L.j, L.k) = y;
+          });
+          if (gl == 0) {
+            double* hp = elem(bx.rhoH, L.i, L.j, L.k);
+            *hp = *hp + P.dt * v.F(NS);
           }
-          double* hp = elem(bx.rhoH, L.i, L.j, L.k);
-          *hp = *hp + P.dt * v.F(NS);
         }
-        if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
-        if (P.status) P.status[cell] = status;
+        if (gl == 0) {
+          if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
+          if (P.status) P.status[cell] = status;
+        }
       }
     }
-    warp_append(live && need == kNeedRhs, slot, R.list_out, R.cnt_out);
-    warp_append(live && need == kNeedSetup, slot, R.list_setup, R.cnt_setup);
-    warp_stats(P.stats, live && need == kDone, status != 0, false, c.cnt);
+    const bool lead = live && gl == 0;
+    warp_append(lead && need == kNeedRhs, slot, R.list_out, R.cnt_out);
+    warp_append(lead && need == kNeedSetup, slot, R.list_setup, R.cnt_setup);
+    warp_stats(P.stats, lead && need == kDone, status != 0, false, c.cnt);
   }
 }
 
