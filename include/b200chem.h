@@ -92,11 +92,13 @@ typedef struct b200chem_opts {
   int32_t lu_fp64;       /* 0: FP32 LU + one FP64 refinement step (default); 1: FP64 LU */
   int32_t warps_per_cta; /* unused; kept for layout stability (set 0)           */
   int32_t verbose;
-  int32_t kernel;        /* 0: auto (group integrator); 1: thread-per-cell (only
-                            species counts with a compiled variant); 2: group
-                            integrator; 3: round-based integrator (rhs / ctrl /
-                            setup kernels over compacted cell lists; species
-                            counts with a compiled variant)                    */
+  int32_t kernel;        /* 0: auto (round-based integrator where the species
+                            count has a compiled variant, else the group
+                            integrator); 1: thread-per-cell (compiled species
+                            counts only); 2: group integrator (any species
+                            count); 3: round-based integrator (rhs / ctrl /
+                            setup kernels over compacted cell lists; compiled
+                            species counts only)                               */
   int32_t setup_ratio;   /* thread-per-cell: a warp runs a Jacobian/LU round when
                             (cells waiting) * setup_ratio >= (cells needing an
                             RHS); 0 = default (2)                                */
@@ -192,6 +194,10 @@ int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* e
 
 /* ReactorBase::close (Source/PeleLMeX.cpp:26). */
 int b200chem_destroy(b200chem_handle h);
+
+/* Number of kernels this handle has launched so far (instrumentation; no
+ * reference counterpart).  -1 for a NULL handle. */
+int64_t b200chem_kernel_launches(b200chem_handle h);
 
 const char* b200chem_last_error(void);
 int b200chem_version(void);

@@ -76,6 +76,8 @@ def load(path: os.PathLike | None = None):
                                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.POINTER(Stats)]
     L.b200chem_destroy.argtypes = [ctypes.c_void_p]
+    L.b200chem_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.b200chem_kernel_launches.restype = ctypes.c_int64
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):
         f = getattr(L, name)
         f.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, _f64p, ctypes.c_void_p]

@@ -208,6 +208,7 @@ struct b200chem_reactor {
   int* h_rcnt = nullptr;     // pinned copy of one counter
   RoundsGrids rgrid{};
   int rgrid_lut = 0;
+  long long launches = 0;  // kernels launched by this handle (instrumentation)
 };
 
 namespace {
@@ -261,6 +262,7 @@ int launch_group(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   if (err) return err;
   Q.gscratch = static_cast<unsigned char*>(h->d_work);
   CK(v->launch(P, Q, (int)grid, smem, st));
+  h->launches++;
   return 0;
 }
 
@@ -282,6 +284,7 @@ int launch_thread_per_cell(b200chem_reactor* h, const ReactParams& P, cudaStream
   Q.nthr = nthr;
   Q.setup_ratio = h->opts.setup_ratio > 0 ? h->opts.setup_ratio : 2;
   CK(tpc_launch(h->N, lut, P, Q, (int)grid, smem, st));
+  h->launches++;
   return 0;
 }
 
@@ -366,6 +369,7 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     R.list_setup = listS;
     R.cnt_setup = cntS;
     CK(rounds_launch(h->N, lut, kRoundsStart, R, h->rgrid, 0, st));
+      h->launches++;
     int* lst[2] = {listA, listB};
     int* cnt[2] = {cntA, cntB};
     int cur = 0;
@@ -378,15 +382,20 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
       R.list_setup = listS;
       R.cnt_setup = cntS;
       CK(rounds_launch(h->N, lut, kRoundsRhs, R, h->rgrid, 0, st));
+      h->launches++;
       CK(cudaMemsetAsync(cnt[1 - cur], 0, sizeof(int), st));
       CK(cudaMemsetAsync(cntS, 0, sizeof(int), st));
       CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 1, st));
+      h->launches++;
       R.list_in = listS;
       R.cnt_in = cntS;
       CK(rounds_launch(h->N, lut, kRoundsJac, R, h->rgrid, 0, st));
+      h->launches++;
       CK(rounds_launch(h->N, lut, kRoundsGj, R, h->rgrid, 0, st));
+      h->launches++;
       // cells coming back from a setup always ask for a right-hand side next
       CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 0, st));
+      h->launches++;
       cur = 1 - cur;
       if ((round + 1) % kRoundsCheckEvery == 0) {
         CK(cudaMemcpyAsync(h->h_rcnt, cnt[cur], sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -438,9 +447,12 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   if (h->opts.kernel == 1 && !tpc_supported(h->N))
     return set_err(B200CHEM_EINVAL, "thread-per-cell kernel requested but not compiled for N=%d", h->N);
   if (total > 0) {
-    const int err = (h->opts.kernel == 1)   ? launch_thread_per_cell(h, P, st)
-                    : (h->opts.kernel == 3) ? launch_rounds(h, P, st)
-                                            : launch_group(h, P, st);
+    // auto: the round-based integrator where its species count is compiled,
+    // else the group integrator (any species count)
+    const int k = (h->opts.kernel == 0) ? (rounds_supported(h->N) ? 3 : 2) : h->opts.kernel;
+    const int err = (k == 1) ? launch_thread_per_cell(h, P, st)
+                    : (k == 3) ? launch_rounds(h, P, st)
+                               : launch_group(h, P, st);
     if (err) return err;
   }
   if (stats) {
@@ -872,6 +884,8 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
   if (time) *time += *dt_react;
   return 0;
 }
+
+int64_t b200chem_kernel_launches(b200chem_handle h) { return h ? h->launches : -1; }
 
 int b200chem_destroy(b200chem_handle h) {
   if (!h) return 0;

@@ -104,20 +104,50 @@ __device__ __forceinline__ unsigned char* rec_of(const RState& S, long long slot
   return S.rec + slot * S.L.stride;
 }
 
+// Field-by-field copies (no address of the local RCell is taken, so its
+// fields can live in registers).
+#define B200_RCELL_SCALARS(X)                                                                              \
+  X(h) X(hprime) X(hscale) X(eta) X(etamax) X(tn) X(gamma) X(gammap) X(gamrat) X(crate) X(acnrm) X(rl1)    \
+  X(saved_tq5) X(gamma_lu) X(dt) X(saved_t) X(delp) X(hg) X(hub) X(hlb) X(q) X(qprime) X(L) X(qwait)      \
+  X(nstlp) X(nstlj) X(jcur) X(ncf) X(nef) X(nflag) X(convfail) X(callSetup) X(jbad) X(mnewt) X(attempt)    \
+  X(count1) X(hnewOK) X(nstloc) X(qmax) X(max_steps) X(setup_conv) X(label) X(setup_ier) X(cnt.nst)       \
+  X(cnt.nfe) X(cnt.nje) X(cnt.nlu) X(cnt.netf) X(cnt.ncfn) X(cnt.nni)
+
 __device__ __forceinline__ void load_cell(RCell& c, const unsigned char* rec) {
-  const uint4* src = reinterpret_cast<const uint4*>(rec);
-  uint4* dst = reinterpret_cast<uint4*>(&c);
+  const RCell* g = reinterpret_cast<const RCell*>(rec);
+#define B200_LD(f) c.f = g->f;
+  B200_RCELL_SCALARS(B200_LD)
+#undef B200_LD
 #pragma unroll
-  for (int k = 0; k < (int)(sizeof(RCell) / 16); ++k) dst[k] = src[k];
+  for (int i = 0; i < kZn + 2; ++i) c.tau[i] = g->tau[i];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) c.tq[i] = g->tq[i];
+#pragma unroll
+  for (int i = 0; i < kZn; ++i) c.l[i] = g->l[i];
 }
 
 __device__ __forceinline__ void store_cell(const RCell& c, unsigned char* rec) {
-  const uint4* src = reinterpret_cast<const uint4*>(&c);
-  uint4* dst = reinterpret_cast<uint4*>(rec);
+  RCell* g = reinterpret_cast<RCell*>(rec);
+#define B200_ST(f) g->f = c.f;
+  B200_RCELL_SCALARS(B200_ST)
+#undef B200_ST
 #pragma unroll
-  for (int k = 0; k < (int)(sizeof(RCell) / 16); ++k) dst[k] = src[k];
+  for (int i = 0; i < kZn + 2; ++i) g->tau[i] = c.tau[i];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) g->tq[i] = c.tq[i];
+#pragma unroll
+  for (int i = 0; i < kZn; ++i) g->l[i] = c.l[i];
 }
 
+// a[k] for a runtime k < N with compile-time indexing (keeps a in registers)
+template <int N>
+__device__ __forceinline__ double sel(const double (&a)[N], int k) {
+  double r = a[0];
+#pragma unroll
+  for (int i = 1; i < N; ++i)
+    if (i == k) r = a[i];
+  return r;
+}
 
 // ------------------------------------------------------- lane groups
 // The control kernel runs G lanes per cell (G = 8 or 16): lane gl of a group
@@ -212,29 +242,38 @@ __device__ __forceinline__ void r_set_bdf(RCell& c) {
   const int q = c.q;
   double xi_inv = 1.0, xistar_inv = 1.0;
   c.l[0] = c.l[1] = 1.0;
-  for (int i = 2; i <= q; ++i) c.l[i] = 0.0;
+#pragma unroll
+  for (int i = 2; i < kZn; ++i)
+    if (i <= q) c.l[i] = 0.0;
   double alpha0 = -1.0, alpha0_hat = -1.0, hsum = c.h;
   if (q > 1) {
-    for (int j = 2; j < q; ++j) {
-      hsum += c.tau[j - 1];
-      xi_inv = c.h / hsum;
-      alpha0 -= 1.0 / j;
-      for (int i = j; i >= 1; --i) c.l[i] += c.l[i - 1] * xi_inv;
+#pragma unroll
+    for (int j = 2; j < kZn; ++j) {
+      if (j < q) {
+        hsum += c.tau[j - 1];
+        xi_inv = c.h / hsum;
+        alpha0 -= 1.0 / j;
+#pragma unroll
+        for (int i = j; i >= 1; --i) c.l[i] += c.l[i - 1] * xi_inv;
+      }
     }
     alpha0 -= 1.0 / q;
     xistar_inv = -c.l[1] - alpha0;
-    hsum += c.tau[q - 1];
+    hsum += sel(c.tau, q - 1);
     xi_inv = c.h / hsum;
     alpha0_hat = -c.l[1] - xi_inv;
-    for (int i = q; i >= 1; --i) c.l[i] += c.l[i - 1] * xistar_inv;
+#pragma unroll
+    for (int i = kZn - 1; i >= 1; --i)
+      if (i <= q) c.l[i] += c.l[i - 1] * xistar_inv;
   }
+  const double lq = sel(c.l, q);
   const double A1 = 1.0 - alpha0_hat + alpha0;
   const double A2 = 1.0 + q * A1;
   c.tq[2] = fabs(A1 / (alpha0 * A2));
-  c.tq[5] = fabs(A2 * xistar_inv / (c.l[q] * xi_inv));
+  c.tq[5] = fabs(A2 * xistar_inv / (lq * xi_inv));
   if (c.qwait == 1) {
     if (q > 1) {
-      const double C = xistar_inv / c.l[q];
+      const double C = xistar_inv / lq;
       const double A3 = alpha0 + 1.0 / q;
       const double A4 = alpha0_hat + xi_inv;
       const double Cpinv = (1.0 - A4 + A3) / A3;
@@ -242,7 +281,7 @@ __device__ __forceinline__ void r_set_bdf(RCell& c) {
     } else {
       c.tq[1] = 1.0;
     }
-    hsum += c.tau[q];
+    hsum += sel(c.tau, q);
     xi_inv = c.h / hsum;
     const double A5 = alpha0 - 1.0 / (q + 1);
     const double A6 = alpha0_hat - xi_inv;
@@ -259,40 +298,65 @@ __device__ __forceinline__ void r_set_bdf(RCell& c) {
 template <int n, int G>
 __device__ __forceinline__ void r_increase(RCell& c, const RVec<n>& v, int gl) {
   const int q = c.q;
-  for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < kZn; ++i)
+    if (i <= c.qmax) c.l[i] = 0.0;
   double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = c.hscale;
   c.l[2] = 1.0;
-  for (int j = 1; j < q; ++j) {
-    hsum += c.tau[j + 1];
-    const double xi = hsum / c.hscale;
-    prod *= xi;
-    alpha0 -= 1.0 / (j + 1);
-    alpha1 += 1.0 / xi;
-    for (int i = j + 2; i >= 2; --i) c.l[i] = c.l[i] * xiold + c.l[i - 1];
-    xiold = xi;
+#pragma unroll
+  for (int j = 1; j < kZn - 1; ++j) {
+    if (j < q) {
+      hsum += c.tau[j + 1];
+      const double xi = hsum / c.hscale;
+      prod *= xi;
+      alpha0 -= 1.0 / (j + 1);
+      alpha1 += 1.0 / xi;
+#pragma unroll
+      for (int i = j + 2; i >= 2; --i)
+        if (i < kZn) c.l[i] = c.l[i] * xiold + c.l[i - 1];
+      xiold = xi;
+    }
   }
   const double A1 = (-alpha0 - alpha1) / prod;
+  const int qm = c.qmax;
+  double lj[kZn];
+#pragma unroll
+  for (int j = 0; j < kZn; ++j) lj[j] = c.l[j];
   each<n, G>(gl, [&](int i) {
-    const double z = A1 * v.zn(c.qmax, i);
+    const double z = A1 * v.zn(qm, i);
     v.zn(q + 1, i) = z;
-    for (int j = 2; j <= q; ++j) v.zn(j, i) += c.l[j] * z;
+#pragma unroll
+    for (int j = 2; j < kZn; ++j)
+      if (j <= q) v.zn(j, i) += lj[j] * z;
   });
 }
 
 template <int n, int G>
 __device__ __forceinline__ void r_decrease(RCell& c, const RVec<n>& v, int gl) {
   const int q = c.q;
-  for (int i = 0; i <= c.qmax; ++i) c.l[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < kZn; ++i)
+    if (i <= c.qmax) c.l[i] = 0.0;
   c.l[2] = 1.0;
   double hsum = 0.0;
-  for (int j = 1; j <= q - 2; ++j) {
-    hsum += c.tau[j];
-    const double xi = hsum / c.hscale;
-    for (int i = j + 2; i >= 2; --i) c.l[i] = c.l[i] * xi + c.l[i - 1];
+#pragma unroll
+  for (int j = 1; j < kZn - 2; ++j) {
+    if (j <= q - 2) {
+      hsum += c.tau[j];
+      const double xi = hsum / c.hscale;
+#pragma unroll
+      for (int i = j + 2; i >= 2; --i)
+        if (i < kZn) c.l[i] = c.l[i] * xi + c.l[i - 1];
+    }
   }
+  double lj[kZn];
+#pragma unroll
+  for (int j = 0; j < kZn; ++j) lj[j] = c.l[j];
   each<n, G>(gl, [&](int i) {
     const double zq = v.zn(q, i);
-    for (int j = 2; j < q; ++j) v.zn(j, i) -= c.l[j] * zq;
+#pragma unroll
+    for (int j = 2; j < kZn; ++j)
+      if (j < q) v.zn(j, i) -= lj[j] * zq;
   });
 }
 
@@ -679,15 +743,22 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         if (dsm <= 1.0) {
           // complete the step
           c.cnt.nst++;
-          for (int i = c.q; i >= 2; --i) c.tau[i] = c.tau[i - 1];
+#pragma unroll
+          for (int i = kZn + 1; i >= 2; --i)
+            if (i <= c.q) c.tau[i] = c.tau[i - 1];
           if (c.q == 1 && c.cnt.nst > 1) c.tau[2] = c.tau[1];
           c.tau[1] = c.h;
           const int q = c.q;
           const bool save = (c.qwait - 1 == 1 && q != c.qmax);
           const int qm = c.qmax;
+          double lj[kZn];
+#pragma unroll
+          for (int j = 0; j < kZn; ++j) lj[j] = c.l[j];
           each<n, G>(gl, [&](int i) {
             const double ac = v.acor(i);
-            for (int j = 0; j <= q; ++j) v.zn(j, i) += c.l[j] * ac;
+#pragma unroll
+            for (int j = 0; j < kZn; ++j)
+              if (j <= q) v.zn(j, i) += lj[j] * ac;
             if (save) v.zn(qm, i) = ac;
           });
           c.qwait--;

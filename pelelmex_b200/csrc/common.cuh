@@ -112,10 +112,10 @@ cudaError_t tpc_launch(int N, int lut_bytes, const ReactParams& P, const TpcPara
 constexpr int kRoundsRhsBlock = 64;  // threads per CTA of the rhs kernel
 enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsJac, kRoundsGj };
 
-// Per-warp scratch of the setup kernels.  Jacobian kernel, shared: C, g/RT,
-// h/RT [Npad], rates [Rpad] (double); global: four per-reaction arrays [Rpad]
-// (double).  Inverse kernel, shared: Dsc [Npad] (double), matrix [n][ldl] and
-// pivot column [Npad] (LUT), two index arrays [Npad] (int).
+// Per-warp shared scratch of the setup kernels.  Jacobian kernel: C, g/RT,
+// h/RT [Npad], rates and four per-reaction Jacobian terms [Rpad] (double).
+// Inverse kernel: Dsc [Npad] (double), matrix [n][ldl] and pivot column
+// [Npad] (LUT), two index arrays [Npad] (int).
 struct RoundsSetupLayout {
   int Npad, Rpad, ldl;
   int jac_smem_per_warp, gj_smem_per_warp;

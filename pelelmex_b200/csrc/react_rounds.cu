@@ -276,6 +276,12 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
   }
 }
 
+// Minimum resident CTAs per SM requested for the control kernel (its
+// register budget: 3 -> 168 registers per thread).
+#ifndef B200_CTRL_MIN_CTAS
+#define B200_CTRL_MIN_CTAS 3
+#endif
+
 // Lanes per cell of the control kernel.
 constexpr int ctrl_group(int n) { return n <= 32 ? 8 : 16; }
 
@@ -283,7 +289,7 @@ constexpr int ctrl_group(int n) { return n <= 32 ? 8 : 16; }
 // the f just evaluated (counted in nfe); otherwise they come back from a
 // setup.
 template <int NS, typename LUT>
-__global__ void __launch_bounds__(128) rk_ctrl(RoundsParams R, int after_rhs) {
+__global__ void __launch_bounds__(128, B200_CTRL_MIN_CTAS) rk_ctrl(RoundsParams R, int after_rhs) {
   constexpr int n = NS + 1;
   constexpr int G = ctrl_group(n);
   constexpr int GPW = 32 / G;  // cells per warp
@@ -433,11 +439,13 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
   ms.gRT = d + SL.Npad;
   ms.hRT = d + 2 * SL.Npad;
   ms.q = d + 3 * SL.Npad;
-  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
-  ms.r1 = reinterpret_cast<double*>(R.wscratch + gw * SL.gbytes_per_warp);
+  // per-reaction Jacobian terms in shared memory too: phase 2 reads them for
+  // every reaction on every lane
+  ms.r1 = ms.q + SL.Rpad;
   ms.r2 = ms.r1 + SL.Rpad;
   ms.r3 = ms.r2 + SL.Rpad;
   ms.r4 = ms.r3 + SL.Rpad;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
   const int cnt = *R.cnt_in;
   const RLayout RL = R.S.L;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -618,7 +626,7 @@ RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
   L.Npad = ((n + 31) / 32) * 32;
   L.Rpad = std::max(32, ((R + 31) / 32) * 32);
   L.ldl = n | 1;
-  L.jac_smem_per_warp = (int)(8LL * (3 * L.Npad + L.Rpad));
+  L.jac_smem_per_warp = (int)(8LL * (3 * L.Npad + 5 * L.Rpad));
   const long long b = 8LL * L.Npad + (long long)lut_bytes * ((long long)n * L.ldl + L.Npad) + 4LL * 2 * L.Npad;
   L.gj_smem_per_warp = (int)((b + 15) & ~15LL);
   L.gbytes_per_warp = (8LL * 4LL * L.Rpad + 255) & ~255LL;

@@ -166,6 +166,11 @@ class ReactorB200:
             arr = (ctypes.c_double * len(typ))(*typ)
             _lib.check(_lib.load().b200chem_set_typvals(self._h, arr, len(typ)))
 
+    def kernel_launches(self) -> int:
+        """Kernels this reactor has launched so far."""
+        self._need()
+        return int(_lib.load().b200chem_kernel_launches(self._h))
+
     def close(self):
         if self._h:
             _lib.load().b200chem_destroy(self._h)

@@ -164,7 +164,7 @@ def test_kernels_group_sizes_and_lu_precisions(kernel, lanes, lu_fp64, orc_cache
 def test_group_sizes_on_h2(lanes, orc_cache):
     """Group sizes on the 10-component system (1 or 2 components per lane)."""
     f = W.premixed_h2(M.builtin("synth_h2_9"), edge=8)
-    g = run_gpu("synth_h2_9", f, group_lanes=lanes)
+    g = run_gpu("synth_h2_9", f, group_lanes=lanes, kernel="group")
     o = orc_cache("synth_h2_9").react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12,
                                       max_order=5)
     compare(f, g, o, f"synth_h2_9 G={lanes}")
