@@ -228,6 +228,21 @@ int b200chem_inst_rr(b200chem_handle h, const double* rhoY_mks, const double* rh
 int b200chem_t_from_hy(b200chem_handle h, const double* rhoY_mks, const double* rhoH_mks,
                        double* T, int64_t ncells, void* stream);
 
+/* ------------------------------------------------------- surrogate MLP
+ * No reference counterpart: the learned part of the reactor (a small MLP
+ * predicting the state change over dt_react, with residual-gated fallback to
+ * the BDF integrator).  BF16 tensor-core GEMM with fused epilogue:
+ *   C[M][N] = epi(A[M][K] . B[N][K]^T + bias[N])
+ * A, B: device BF16, row-major, K contiguous, 16-byte aligned rows (lda, ldb
+ * multiples of 8); M % 128 == 0, N % 16 == 0 (N <= 256 or N % 256 == 0),
+ * K % 16 == 0.  epi: 0 C fp32; 1 C bf16; 2 C bf16 = gelu(.), aux fp32 =
+ * pre-activation (aux may be NULL); 3 C bf16 = (A.B^T) * gelu'(aux).  Only
+ * columns < n_valid (0 = N) of C are written.  *err (device int, optional)
+ * is set to 1 if a tensor-core completion wait timed out. */
+int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K,
+                           void* C, long long ldc, const float* bias, float* aux, int epi, int n_valid, int* err,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,11 @@ def load(path: os.PathLike | None = None):
                                       ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.POINTER(Stats)]
     L.b200chem_destroy.argtypes = [ctypes.c_void_p]
+    L.b200chem_mlp_gemm_bf16.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_longlong,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+    L.b200chem_mlp_gemm_bf16.restype = ctypes.c_int
     L.b200chem_kernel_launches.argtypes = [ctypes.c_void_p]
     L.b200chem_kernel_launches.restype = ctypes.c_int64
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):

@@ -1,0 +1,334 @@
+// mlp_tc.cu -- BF16 tensor-core (tcgen05) GEMM with fused epilogues for the
+// chemistry surrogate MLP (inference and training), plus the elementwise
+// kernels of its training step.
+//
+//   C[M, N] = epi(A[M, K] . B[N, K]^T + bias[N])
+//
+// A and B are BF16, row-major with K contiguous ("K-major" for both UMMA
+// operands).  One CTA of 128 threads owns a 128-row tile of C at a time
+// (persistent over tiles).  Operand tiles are staged by the CTA's threads into
+// shared memory in the UMMA canonical no-swizzle K-major layout: 8-row x
+// 16-byte core matrices, core matrices of one 8-row group contiguous along K
+// (LBO = 128 B), row groups SBO = KC / 8 * 128 B apart.  One thread issues
+// tcgen05.mma (kind::f16, M = 128, N = the N tile, K = 16 per instruction)
+// accumulating in tensor memory (FP32, 128 lanes x N columns);
+// tcgen05.commit signals an mbarrier when the MMAs are done; each warp then
+// reads its 32 lanes (rows) of the accumulator with tcgen05.ld and applies
+// the epilogue.  When K and N fit (K <= 256, N <= 256) B is staged once per
+// CTA and stays resident across row tiles (the weights of one layer);
+// otherwise B is re-staged per K chunk.
+//
+// Every wait on the mbarrier is bounded; on timeout the kernel raises a flag
+// in err (read by the host) and stops issuing work.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace b200 {
+namespace mlp {
+
+constexpr int kTileM = 128;
+constexpr int kThreads = 128;
+
+enum Epilogue : int {
+  kEpiF32 = 0,        // C fp32 = acc + bias
+  kEpiBf16 = 1,       // C bf16 = acc + bias
+  kEpiGeluBf16 = 2,   // C bf16 = gelu(acc + bias); aux fp32 = acc + bias (pre-activation, may be null)
+  kEpiDGeluBf16 = 3,  // C bf16 = acc * gelu'(aux[pre-activation])  (backward through GELU)
+};
+
+struct GemmArgs {
+  const __nv_bfloat16* A;
+  const __nv_bfloat16* B;
+  long long lda, ldb;  // row strides (elements)
+  int M, N, K;         // M % 128 == 0, N % 16 == 0, K % 16 == 0
+  void* C;
+  long long ldc;
+  const float* bias;   // [N] or null
+  float* aux;          // epilogue side input/output [M][ldc]
+  int epi;
+  int n_valid;         // columns of C actually written (<= N)
+  int* err;            // raised on an mbarrier timeout
+};
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory matrix descriptor, no swizzle, K-major.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for this architecture
+  // base offset 0, legacy LBO mode, layout type 0 = no swizzle
+  return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, both operands K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4)                          // D format F32
+         | (1u << 7)                        // A format BF16
+         | (1u << 10)                       // B format BF16
+         | ((uint32_t)(N >> 3) << 17)       // N / 8
+         | ((uint32_t)(M >> 4) << 24);      // M / 16
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false after ~2^22 polls (seconds) without completion.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (mbar_try_wait(bar, phase)) return true;
+    if (i > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's lane (row).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ------------------------------------------------------------ staging
+// rows x kc block of a K-contiguous bf16 matrix into the canonical layout:
+// element (r, k) at (r / 8) * (kc / 8) * 128 + (k / 8) * 128 + (r % 8) * 16
+// + (k % 8) * 2 bytes.  Rows >= rows_valid are zero.  16-byte copies.
+__device__ __forceinline__ void stage_tile(unsigned char* dst, const __nv_bfloat16* src, long long ld, int rows,
+                                           int rows_valid, int k0, int kc) {
+  const int chunks_per_row = kc / 8;
+  const int total = rows * chunks_per_row;
+  for (int c = threadIdx.x; c < total; c += blockDim.x) {
+    const int r = c / chunks_per_row, kb = c % chunks_per_row;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (r < rows_valid) v = *reinterpret_cast<const uint4*>(src + (long long)r * ld + k0 + kb * 8);
+    const int off = (r >> 3) * chunks_per_row * 128 + kb * 128 + (r & 7) * 16;
+    *reinterpret_cast<uint4*>(dst + off) = v;
+  }
+}
+
+__device__ __forceinline__ float gelu(float x) {
+  // tanh form of GELU (Hendrycks & Gimpel 2016)
+  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+  return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
+}
+
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+  const float u = k0 * (x + k1 * x * x * x);
+  const float t = tanhf(u);
+  const float du = k0 * (1.0f + 3.0f * k1 * x * x);
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
+}
+
+// ------------------------------------------------------------ GEMM kernel
+__global__ void __launch_bounds__(kThreads, 1) gemm_bf16_tc(GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int abort_s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool resident = (g.K <= 256 && g.N <= 256);
+  const int NT = g.N <= 256 ? g.N : 256;          // N tile
+  const int KC = resident ? g.K : 64;             // K chunk
+  unsigned char* As = smem;                        // [128 x KC]
+  unsigned char* Bs = smem + kTileM * KC * 2;      // [NT x KC]
+  const uint32_t ncols = NT <= 32 ? 32 : (NT <= 64 ? 64 : (NT <= 128 ? 128 : 256));
+  if (warp == 0) tmem_alloc(&tmem_base_s, ncols);
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t idesc = umma_idesc_bf16(kTileM, NT);
+  const int mtiles = g.M / kTileM, ntiles = (g.N + NT - 1) / NT;
+  uint32_t phase = 0;
+  bool b_loaded = false;
+  for (int t = blockIdx.x; t < mtiles * ntiles; t += gridDim.x) {
+    const int mt = t / ntiles, nt = t % ntiles;
+    const int n0 = nt * NT;
+    for (int k0 = 0; k0 < g.K; k0 += KC) {
+      stage_tile(As, g.A + (long long)mt * kTileM * g.lda, g.lda, kTileM, kTileM, k0, KC);
+      if (!resident || !b_loaded) stage_tile(Bs, g.B + (long long)n0 * g.ldb, g.ldb, NT, NT, k0, KC);
+      b_loaded = true;
+      fence_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+        const uint32_t sbo = (uint32_t)(KC / 8) * 128u;
+        for (int ks = 0; ks < KC / 16; ++ks) {
+          const uint64_t ad = umma_desc(a0 + ks * 256u, 128u, sbo);
+          const uint64_t bd = umma_desc(b0 + ks * 256u, 128u, sbo);
+          umma_bf16(tmem, ad, bd, idesc, (k0 > 0 || ks > 0) ? 1u : 0u);
+        }
+        umma_commit(&bar);
+      }
+      // the staged operands are reused only after the MMAs that read them are done
+      const bool ok = mbar_wait_bounded(&bar, phase);
+      phase ^= 1u;
+      if (!ok) abort_s = 1;
+      __syncthreads();
+      if (abort_s) break;
+    }
+    if (abort_s) break;
+    tc_fence_after();
+    // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w + 31
+    const int row = mt * kTileM + warp * 32 + lane;
+    for (int c0 = 0; c0 < NT; c0 += 32) {
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      const int col0 = n0 + c0;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int col = col0 + i;
+        if (col < g.n_valid && g.bias) v[i] += __ldg(g.bias + col);
+      }
+      if (g.epi == kEpiF32) {
+        float* C = reinterpret_cast<float*>(g.C) + (long long)row * g.ldc;
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col0 + i < g.n_valid) C[col0 + i] = v[i];
+      } else {
+        __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (long long)row * g.ldc;
+        if (g.epi == kEpiGeluBf16) {
+          float* P = g.aux ? g.aux + (long long)row * g.ldc : nullptr;
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            if (P && col0 + i < g.n_valid) P[col0 + i] = v[i];
+            v[i] = gelu(v[i]);
+          }
+        } else if (g.epi == kEpiDGeluBf16) {
+          const float* P = g.aux + (long long)row * g.ldc;
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (col0 + i < g.n_valid) v[i] *= gelu_grad(P[col0 + i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (col0 + i < g.n_valid) C[col0 + i] = __float2bfloat16_rn(v[i]);
+      }
+    }
+    // all warps have read the accumulator before the next tile overwrites it
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (abort_s && tid == 0 && g.err) atomicExch(g.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+}  // namespace mlp
+}  // namespace b200
+
+// ------------------------------------------------------------------ C ABI
+using namespace b200::mlp;
+
+extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K,
+                                      void* C, long long ldc, const float* bias, float* aux, int epi, int n_valid,
+                                      int* err, void* stream) {
+  if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return -1;
+  if (M % kTileM || N % 16 || K % 16 || (N > 256 && N % 256)) return -1;
+  if (epi < kEpiF32 || epi > kEpiDGeluBf16) return -1;
+  if (epi == kEpiDGeluBf16 && !aux) return -1;
+  if (lda % 8 || ldb % 8) return -1;  // 16-byte staging loads
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return -1;
+  GemmArgs g;
+  g.A = static_cast<const __nv_bfloat16*>(A);
+  g.B = static_cast<const __nv_bfloat16*>(B);
+  g.lda = lda;
+  g.ldb = ldb;
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.C = C;
+  g.ldc = ldc;
+  g.bias = bias;
+  g.aux = aux;
+  g.epi = epi;
+  g.n_valid = n_valid > 0 ? n_valid : N;
+  g.err = err;
+  const bool resident = (K <= 256 && N <= 256);
+  const int NT = N <= 256 ? N : 256;
+  const int KC = resident ? K : 64;
+  const int smem = kTileM * KC * 2 + NT * KC * 2;
+  cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return -2;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int tiles = (M / kTileM) * ((N + NT - 1) / NT);
+  const int grid = tiles < sms ? tiles : sms;
+  gemm_bf16_tc<<<grid, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}

@@ -1,0 +1,85 @@
+"""tcgen05 BF16 GEMM of the surrogate MLP against a plain PyTorch FP32 matmul
+of the same BF16 operands (FP32 accumulation on both sides)."""
+import ctypes
+
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from pelelmex_b200 import _lib  # noqa: E402
+
+DEV = "cuda:0"
+EPI_F32, EPI_BF16, EPI_GELU, EPI_DGELU = 0, 1, 2, 3
+
+
+def gelu(x):
+    return 0.5 * x * (1.0 + torch.tanh(0.7978845608028654 * (x + 0.044715 * x ** 3)))
+
+
+def gelu_grad(x):
+    u = 0.7978845608028654 * (x + 0.044715 * x ** 3)
+    t = torch.tanh(u)
+    return 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * 0.7978845608028654 * (1 + 3 * 0.044715 * x * x)
+
+
+def gemm(A, B, bias=None, epi=EPI_F32, aux=None, n_valid=0):
+    M, K = A.shape
+    N = B.shape[0]
+    out = torch.empty((M, N), device=DEV, dtype=torch.float32 if epi == EPI_F32 else torch.bfloat16)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    L = _lib.load()
+    code = L.b200chem_mlp_gemm_bf16(A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), M, N, K, out.data_ptr(),
+                                    out.stride(0), bias.data_ptr() if bias is not None else None,
+                                    aux.data_ptr() if aux is not None else None, epi, n_valid, err.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream)
+    assert code == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0, "mbarrier wait timed out"
+    return out
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 16, 16), (128, 32, 32), (256, 256, 256), (384, 32, 256), (256, 256, 1024),
+                                   (128, 512, 64), (1024, 256, 32)])
+def test_gemm_f32_matches_torch(M, N, K):
+    g = torch.Generator(device=DEV).manual_seed(M * 7 + N * 3 + K)
+    A = torch.randn((M, K), device=DEV, generator=g).to(torch.bfloat16)
+    B = torch.randn((N, K), device=DEV, generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device=DEV, generator=g)
+    C = gemm(A, B, bias)
+    ref = A.float() @ B.float().T + bias
+    tol = 1e-4 * (K ** 0.5) * ref.abs().max().item()
+    assert (C - ref).abs().max().item() <= tol
+
+
+def test_gemm_epilogues():
+    M, N, K = 256, 256, 256
+    g = torch.Generator(device=DEV).manual_seed(5)
+    A = (0.2 * torch.randn((M, K), device=DEV, generator=g)).to(torch.bfloat16)
+    B = (0.2 * torch.randn((N, K), device=DEV, generator=g)).to(torch.bfloat16)
+    bias = torch.randn(N, device=DEV, generator=g)
+    z = A.float() @ B.float().T + bias
+    pre = torch.empty((M, N), device=DEV, dtype=torch.float32)
+    y = gemm(A, B, bias, EPI_GELU, aux=pre)
+    assert torch.allclose(pre, z, atol=1e-3, rtol=1e-3)
+    assert torch.allclose(y.float(), gelu(z), atol=2e-2, rtol=1e-2)
+    yb = gemm(A, B, bias, EPI_BF16)
+    assert torch.allclose(yb.float(), z, atol=2e-2, rtol=1e-2)
+    d = gemm(A, B, None, EPI_DGELU, aux=pre)
+    ref = (A.float() @ B.float().T) * gelu_grad(pre)
+    assert torch.allclose(d.float(), ref, atol=2e-2, rtol=1e-2)
+
+
+def test_gemm_partial_columns():
+    M, N, K = 128, 32, 256
+    A = torch.randn((M, K), device=DEV).to(torch.bfloat16)
+    B = torch.randn((N, K), device=DEV).to(torch.bfloat16)
+    C = torch.full((M, N), 7.0, device=DEV)
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    code = _lib.load().b200chem_mlp_gemm_bf16(A.data_ptr(), K, B.data_ptr(), K, M, N, K, C.data_ptr(), N, None, None,
+                                               EPI_F32, 22, err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert code == 0
+    torch.cuda.synchronize()
+    ref = A.float() @ B.float().T
+    assert torch.allclose(C[:, :22], ref[:, :22], atol=1e-2, rtol=1e-3)
+    assert torch.all(C[:, 22:] == 7.0)
