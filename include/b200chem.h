@@ -243,6 +243,42 @@ int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* B, long lon
                            void* C, long long ldc, const float* bias, float* aux, int epi, int n_valid, int* err,
                            void* stream);
 
+/* Acceptance thresholds of a surrogate prediction (b200chem_surrogate_gate). */
+typedef struct b200chem_gate_opts {
+  double rtol;      /* relative tolerance of the one-step implicit residual        */
+  double atol;      /* absolute tolerance, times rho (species) or T (temperature) */
+  double tol_T;     /* |T(h, Y_pred) - (T0 + dT_pred)| bound, K                     */
+  double tol_elem;  /* element-conservation bound, relative to the atom content   */
+  double tol_mass;  /* |sum Y_pred - 1| bound (and most negative Y tolerated)     */
+  double rchange;   /* residual tolerance relative to the step change |y1 - y0|   */
+  double dT_max;    /* > 0: predictions with |dT| above it are rejected, K         */
+  int32_t t_source; /* accepted T: 0 from (h, Y) (energy exact), 1 predicted      */
+  int32_t residual_t_only; /* 1: the residual test covers the temperature only   */
+} b200chem_gate_opts;
+
+/* Network input of the surrogate for ncells cells (component-major CGS rhoY
+ * [N][ncells], T [ncells]): x_bf16 [nrows][in] with in = N + 2 rounded up to a
+ * multiple of 16, rows ncells..nrows-1 zero; nrows % 128 == 0.  Columns:
+ * (T, log10(Y_k + 1e-20), log10 dt), each standardised by xmean/xstd [N + 2]. */
+int b200chem_surrogate_features(b200chem_handle h, const double* rhoY, const double* T, int64_t ncells,
+                                int64_t nrows, double dt, const float* xmean, const float* xstd, void* x_bf16,
+                                void* stream);
+
+/* Acceptance gate of a surrogate prediction (pred [ncells][out] FP32,
+ * out = N + 1 rounded up to a multiple of 16, standardised; ymean/ystd
+ * [N + 1]): mass and element conservation of the raw prediction (then an
+ * exact element-conserving correction), T from (h, Y) against the predicted
+ * dT, and (rtol > 0) a one-step implicit residual with two right-hand sides.
+ * Accepted cells are advanced in place (rhoY, T, rhoH, fctCount) and get
+ * accept[c] = 1; the others are left untouched with accept[c] = -(first
+ * failed check): -1 mass, -2 elements, -3 energy, -4 residual, -5 change
+ * cap.  elem
+ * [n_elements][N] holds the atoms of each element in each species. */
+int b200chem_surrogate_gate(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T, double* rhoH,
+                            const double* extF_rhoH, double* fctCount, int64_t ncells, double dt, const float* pred,
+                            const float* ymean, const float* ystd, const double* elem, int32_t n_elements,
+                            const b200chem_gate_opts* opts, int32_t* accept, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,12 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class GateOpts(ctypes.Structure):
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("tol_T", ctypes.c_double),
+                ("tol_elem", ctypes.c_double), ("tol_mass", ctypes.c_double), ("rchange", ctypes.c_double),
+                ("dT_max", ctypes.c_double), ("t_source", ctypes.c_int32), ("residual_t_only", ctypes.c_int32)]
+
+
 class B200ChemError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"b200chem error {code}: {msg}")
@@ -81,6 +87,15 @@ def load(path: os.PathLike | None = None):
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_mlp_gemm_bf16.restype = ctypes.c_int
+    L.b200chem_surrogate_features.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, ctypes.c_int64,
+                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p]
+    L.b200chem_surrogate_features.restype = ctypes.c_int
+    L.b200chem_surrogate_gate.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                          ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                          ctypes.POINTER(GateOpts), ctypes.c_void_p, ctypes.c_void_p]
+    L.b200chem_surrogate_gate.restype = ctypes.c_int
     L.b200chem_kernel_launches.argtypes = [ctypes.c_void_p]
     L.b200chem_kernel_launches.restype = ctypes.c_int64
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):

@@ -211,6 +211,16 @@ struct b200chem_reactor {
   long long launches = 0;  // kernels launched by this handle (instrumentation)
 };
 
+namespace b200 {
+// Accessors for the other translation units (surrogate kernels).
+const DevMech* handle_mech(b200chem_handle h) { return &h->mech; }
+int handle_species(b200chem_handle h) { return h->N; }
+const double* handle_atol(b200chem_handle h) { return h->d_atol; }
+int handle_device(b200chem_handle h) { return h->device; }
+void handle_count_launch(b200chem_handle h) { h->launches++; }
+int handle_set_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+}  // namespace b200
+
 namespace {
 
 template <typename T>
@@ -886,6 +896,7 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
 }
 
 int64_t b200chem_kernel_launches(b200chem_handle h) { return h ? h->launches : -1; }
+
 
 int b200chem_destroy(b200chem_handle h) {
   if (!h) return 0;

@@ -141,6 +141,14 @@ struct RoundsGrids {
   int start, rhs, ctrl, jac, gj;
 };
 
+// Handle accessors (defined with the handle in b200chem.cu).
+const DevMech* handle_mech(b200chem_handle h);
+int handle_species(b200chem_handle h);
+const double* handle_atol(b200chem_handle h);
+int handle_device(b200chem_handle h);
+void handle_count_launch(b200chem_handle h);
+int handle_set_error(int code, const char* msg);
+
 bool rounds_supported(int N);
 RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes);
 long long rounds_state_bytes_per_cell(int N, int lut_bytes);
