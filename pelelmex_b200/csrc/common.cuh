@@ -113,7 +113,7 @@ constexpr int kRoundsRhsBlock = 64;  // threads per CTA of the rhs kernel
 enum { kRoundsStart = 0, kRoundsRhs, kRoundsCtrl, kRoundsJac, kRoundsGj };
 
 // Per-warp shared scratch of the setup kernels.  Jacobian kernel: C, g/RT,
-// h/RT [Npad], rates and four per-reaction Jacobian terms [Rpad] (double).
+// h/RT, third-body row [Npad] and the Jacobian [n][n] (double).
 // Inverse kernel: Dsc [Npad] (double), matrix [n][ldl] and pivot column
 // [Npad] (LUT), two index arrays [Npad] (int).
 struct RoundsSetupLayout {

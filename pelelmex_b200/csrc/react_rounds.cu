@@ -421,6 +421,126 @@ __device__ __forceinline__ int reg_gj_inverse(const double* J, int ldj, const do
   return 0;
 }
 
+// Analytic Jacobian of one cell by one warp, lane per reaction: each lane
+// evaluates its reactions (rates and their derivatives) and adds their
+// contributions to a shared-memory Jacobian with atomics -- the mass-action
+// columns of the reaction's own species, the temperature column, and the
+// third-body terms (the default efficiency 1 of every species as a row
+// vector u added to all columns at the end, the non-default ones per
+// species).  Then lane l finishes column l (mass units) and its temperature
+// row entry, and writes the column into the cell record (column-major, ldj).
+// s: C, g/RT, h/RT [Npad]; Js: [n][n] column-major; us: [Npad] (shared).
+template <int CPL>
+__device__ __forceinline__ void warp_jac(const DevMech& m, const GrpScratch& s, double* Js, double* us,
+                                         const Vec<CPL>& y, const Vec<CPL>& fy, double* J, int ldj, int lane) {
+  const Grp<32> g(lane);
+  const int N = m.N, R = m.R, n = N + 1;
+  const double T = grp_get_T<32, CPL>(g, y, N);
+  const double lnT = log(T), invT = 1.0 / T;
+  double cpk[CPL], hk[CPL], dcpk[CPL];
+  grp_species<32, CPL>(m, s, g, y, T, lnT, cpk, hk, dcpk);
+  double csum = 0.0;
+#pragma unroll
+  for (int c = 0; c < CPL; ++c)
+    if (lane + 32 * c < N) csum += y.v[c] * __ldg(m.inv_mw + lane + 32 * c);
+  const double Ctot = g.sum(csum);
+  const double lnPRT = log(kPatm / (kRu * T));
+  for (int e = lane; e < n * n; e += 32) Js[e] = 0.0;
+  for (int k = lane; k < n; k += 32) us[k] = 0.0;
+  __syncwarp();
+  for (int j = lane; j < R; j += 32) {
+    const RxnEval e = eval_reaction<true>(m, SpView{s.C, s.gRT, s.hRT}, j, T, lnT, invT, Ctot, lnPRT);
+    const int type = __ldg(m.rtype + j);
+    const double mult = (type == 1) ? e.M : 1.0;
+    double ceff = 0.0;
+    if (type == 1) ceff = e.kf * e.pf - e.kr * e.pr;
+    else if (type >= 2) ceff = e.dkf_dM * (e.pf - (e.kf > 0.0 ? e.kr / e.kf : 0.0) * e.pr);
+    const double kfm = mult * e.kf, krm = mult * e.kr;
+    const double dqdT = mult * (e.kf * e.dlnkf_dT * e.pf - e.dkr_dT * e.pr);
+    int sp[8], nu[8];
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+      sp[sl] = __ldg(m.sp + sl * R + j);
+      nu[sl] = __ldg(m.nu + sl * R + j);
+    }
+    // mass-action columns: reactant slots (forward), product slots (reverse)
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      if (sp[a] < 0) continue;
+      const int va = (a < 4) ? -nu[a] : nu[a];
+      double p = va * ipow(s.C[sp[a]], va - 1);
+      const int b0 = (a < 4) ? 0 : 4;
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2) {
+        const int o = b0 + s2;
+        if (o != a && sp[o] >= 0) p *= ipow(s.C[sp[o]], (a < 4) ? -nu[o] : nu[o]);
+      }
+      const double d = (a < 4) ? kfm * p : -krm * p;
+      double* col = Js + sp[a] * n;
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (sp[r] >= 0) atomicAdd(col + sp[r], (double)nu[r] * d);
+    }
+    // temperature column and third-body terms
+    double* colT = Js + N * n;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      if (sp[r] < 0) continue;
+      atomicAdd(colT + sp[r], (double)nu[r] * dqdT);
+      if (type != 0) atomicAdd(us + sp[r], (double)nu[r] * ceff);
+    }
+    if (type != 0) {
+      const int q0 = __ldg(m.eff_ptr + j), q1 = __ldg(m.eff_ptr + j + 1);
+      for (int q = q0; q < q1; ++q) {
+        double* col = Js + __ldg(m.eff_sp + q) * n;
+        const double d = __ldg(m.eff_m1 + q) * ceff;
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (sp[r] >= 0) atomicAdd(col + sp[r], (double)nu[r] * d);
+      }
+    }
+  }
+  // every lane is done with h/RT (read by the reaction derivatives) before it
+  // is overwritten with the mass-specific enthalpy
+  __syncwarp();
+  // temperature-row ingredients
+  double rcp = 0.0, drcp = 0.0, cpdot = 0.0, Tdot = 0.0;
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) {
+    const int k = lane + 32 * c;
+    if (k < N) {
+      rcp += y.v[c] * cpk[c];
+      drcp += y.v[c] * dcpk[c];
+      cpdot += cpk[c] * fy.v[c];
+      s.hRT[k] = hk[c];  // mass-specific h for the temperature row
+    } else if (k == N) {
+      Tdot = fy.v[c];
+    }
+  }
+  rcp = g.sum(rcp);
+  drcp = g.sum(drcp);
+  cpdot = g.sum(cpdot);
+  Tdot = g.sum(Tdot);
+  __syncwarp();
+  // lane l finishes column l: mass units, default third-body row, T row
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) {
+    const int l = lane + 32 * c;
+    if (l > N) continue;
+    const double inv_wl = (l < N) ? __ldg(m.inv_mw + l) : 1.0;
+    const double* src = Js + l * n;
+    double* dst = J + l * ldj;
+    double sum = 0.0;
+    for (int k = 0; k < N; ++k) {
+      const double v = (src[k] + ((l < N) ? us[k] : 0.0)) * __ldg(m.mw + k) * inv_wl;
+      dst[k] = v;
+      sum += s.hRT[k] * v;
+    }
+    dst[N] = -(sum + ((l < N) ? Tdot * cpk[c] : cpdot + Tdot * drcp)) / rcp;
+  }
+  __syncwarp();
+}
+
 // Jacobian refresh for the cells of the setup list whose matrix CVODE's
 // jbad rule marks stale: the analytic FP64 Jacobian (column-major) into the
 // cell record, one warp per cell.
@@ -438,13 +558,9 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
   ms.C = d;
   ms.gRT = d + SL.Npad;
   ms.hRT = d + 2 * SL.Npad;
-  ms.q = d + 3 * SL.Npad;
-  // per-reaction Jacobian terms in shared memory too: phase 2 reads them for
-  // every reaction on every lane
-  ms.r1 = ms.q + SL.Rpad;
-  ms.r2 = ms.r1 + SL.Rpad;
-  ms.r3 = ms.r2 + SL.Rpad;
-  ms.r4 = ms.r3 + SL.Rpad;
+  double* us = d + 3 * SL.Npad;
+  double* Js = d + 4 * SL.Npad;
+  ms.q = ms.r1 = ms.r2 = ms.r3 = ms.r4 = nullptr;
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + w;
   const int cnt = *R.cnt_in;
   const RLayout RL = R.S.L;
@@ -466,8 +582,7 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
         y.v[cc] = (i < n) ? v.yev(i) : 0.0;
         fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
       }
-      grp_jac<32, CPL>(&s_mech, ms, y, fy, reinterpret_cast<double*>(rec + RL.off_j), RL.ldj, lane);
-      __syncwarp();
+      warp_jac<CPL>(s_mech, ms, Js, us, y, fy, reinterpret_cast<double*>(rec + RL.off_j), RL.ldj, lane);
       if (lane == 0) {
         cp->cnt.nje++;
         cp->nstlj = nst;
@@ -626,7 +741,7 @@ RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
   L.Npad = ((n + 31) / 32) * 32;
   L.Rpad = std::max(32, ((R + 31) / 32) * 32);
   L.ldl = n | 1;
-  L.jac_smem_per_warp = (int)(8LL * (3 * L.Npad + 5 * L.Rpad));
+  L.jac_smem_per_warp = (int)(8LL * (4 * L.Npad + (long long)n * n));
   const long long b = 8LL * L.Npad + (long long)lut_bytes * ((long long)n * L.ldl + L.Npad) + 4LL * 2 * L.Npad;
   L.gj_smem_per_warp = (int)((b + 15) & ~15LL);
   L.gbytes_per_warp = (8LL * 4LL * L.Rpad + 255) & ~255LL;
