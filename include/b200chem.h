@@ -98,7 +98,11 @@ typedef struct b200chem_opts {
                             counts only); 2: group integrator (any species
                             count); 3: round-based integrator (rhs / ctrl /
                             setup kernels over compacted cell lists; compiled
-                            species counts only)                               */
+                            species counts only).  The round-based integrator
+                            keeps the mechanism's reaction table in a constant
+                            bank shared by every handle of the process on a
+                            device: react calls of handles with DIFFERENT
+                            mechanisms must not overlap in time.              */
   int32_t setup_ratio;   /* thread-per-cell: a warp runs a Jacobian/LU round when
                             (cells waiting) * setup_ratio >= (cells needing an
                             RHS); 0 = default (2)                                */

@@ -209,6 +209,8 @@ struct b200chem_reactor {
   RoundsGrids rgrid{};
   int rgrid_lut = 0;
   long long launches = 0;  // kernels launched by this handle (instrumentation)
+  unsigned char* h_cmech = nullptr;  // pinned packed constant-memory table (null: too large)
+  int cmech_bytes = 0;
 };
 
 namespace b200 {
@@ -367,6 +369,9 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   int* cntB = h->d_rcnt + 1;
   int* cntS = h->d_rcnt + 2;
   R.wscratch = static_cast<unsigned char*>(h->d_rwarp);
+  // the right-hand side reads the mechanism from the constant bank when it fits
+  R.const_mech = h->cmech_bytes > 0 ? 1 : 0;
+  if (R.const_mech) CK(rounds_upload_const(h->h_cmech, h->cmech_bytes, st));
   const long long max_rounds = 64LL * std::max(1, (int)h->opts.max_steps) + 1024;
   for (long long chunk0 = 0; chunk0 < P.total; chunk0 += cap) {
     R.chunk0 = chunk0;
@@ -604,6 +609,66 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
     }
   }
   incptr[N] = (int)incrxn.size();
+  // packed constant-memory table of the round integrator's right-hand side
+  std::vector<unsigned char> cblob;
+  {
+    auto al = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    CMechHeader hd{};
+    hd.N = N;
+    hd.R = R;
+    hd.n_eff = (int)effsp.size();
+    size_t off = al(sizeof(CMechHeader));
+    hd.off_nasa = (int)off;
+    off = al(off + sizeof(double) * nasa.size());
+    hd.off_mw = (int)off;
+    off = al(off + sizeof(double) * N);
+    hd.off_imw = (int)off;
+    off = al(off + sizeof(double) * N);
+    hd.off_rxn = (int)off;
+    off = al(off + sizeof(RxnC) * (size_t)R);
+    hd.off_effsp = (int)off;
+    off = al(off + sizeof(short) * std::max<size_t>(effsp.size(), 1));
+    hd.off_effm1 = (int)off;
+    off = al(off + sizeof(double) * std::max<size_t>(effm1.size(), 1));
+    hd.bytes = (int)off;
+    if (off <= (size_t)kConstMechBytes && N < 128) {
+      cblob.assign(off, 0);
+      memcpy(cblob.data(), &hd, sizeof(hd));
+      memcpy(cblob.data() + hd.off_nasa, nasa.data(), sizeof(double) * nasa.size());
+      memcpy(cblob.data() + hd.off_mw, mw.data(), sizeof(double) * N);
+      memcpy(cblob.data() + hd.off_imw, imw.data(), sizeof(double) * N);
+      RxnC* rx = reinterpret_cast<RxnC*>(cblob.data() + hd.off_rxn);
+      for (int j = 0; j < R; ++j) {
+        RxnC r{};
+        r.lnA = arr[j];
+        r.b = arr[(size_t)R + j];
+        r.ea = arr[2 * (size_t)R + j];
+        r.lnA0 = arrlo[j];
+        r.b0 = arrlo[(size_t)R + j];
+        r.ea0 = arrlo[2 * (size_t)R + j];
+        r.ta = troe[j];
+        r.t3i = troe[(size_t)R + j];
+        r.t1i = troe[2 * (size_t)R + j];
+        r.t2 = troe[3 * (size_t)R + j];
+        r.sdnu = sdnu[j];
+        r.lr = arrrev[j];
+        r.br = arrrev[(size_t)R + j];
+        r.er = arrrev[2 * (size_t)R + j];
+        for (int sl = 0; sl < 8; ++sl) {
+          r.sp[sl] = (signed char)sp[(size_t)sl * R + j];
+          r.nu[sl] = (signed char)nu[(size_t)sl * R + j];
+        }
+        r.type = (short)rtype[j];
+        r.flags = (short)rflags[j];
+        r.e0 = (short)effptr[j];
+        r.e1 = (short)effptr[j + 1];
+        rx[j] = r;
+      }
+      short* es = reinterpret_cast<short*>(cblob.data() + hd.off_effsp);
+      for (size_t q = 0; q < effsp.size(); ++q) es[q] = (short)effsp[q];
+      memcpy(cblob.data() + hd.off_effm1, effm1.data(), sizeof(double) * effm1.size());
+    }
+  }
   std::vector<unsigned char> buf;
   size_t o_mw = push(buf, mw), o_imw = push(buf, imw), o_nasa = push(buf, nasa), o_rtype = push(buf, rtype),
          o_rflags = push(buf, rflags), o_arr = push(buf, arr), o_arrlo = push(buf, arrlo),
@@ -652,6 +717,11 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
   m.inc_ptr = reinterpret_cast<const int*>(base + o_incptr);
   m.inc_rxn = reinterpret_cast<const int*>(base + o_incrxn);
   m.inc_nu = reinterpret_cast<const double*>(base + o_incnu);
+  if (!cblob.empty()) {
+    if ((e = cudaMallocHost(&h->h_cmech, cblob.size())) != cudaSuccess) return fail(e, "cudaMallocHost(table)");
+    memcpy(h->h_cmech, cblob.data(), cblob.size());
+    h->cmech_bytes = (int)cblob.size();
+  }
   h->atol_host.assign(h->n, o->atol);
   if ((e = cudaMalloc(&h->d_atol, sizeof(double) * h->n)) != cudaSuccess) return fail(e, "cudaMalloc(atol)");
   if ((e = cudaMemcpy(h->d_atol, h->atol_host.data(), sizeof(double) * h->n, cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -912,6 +982,7 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->d_rwarp) cudaFree(h->d_rwarp);
   if (h->d_rcnt) cudaFree(h->d_rcnt);
   if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
+  if (h->h_cmech) cudaFreeHost(h->h_cmech);
   delete h;
   return 0;
 }

@@ -135,6 +135,7 @@ struct RoundsParams {
   int* list_setup;   // cells that need a Newton-matrix setup this round
   int* cnt_setup;
   unsigned char* wscratch;  // [setup warps][SL.gbytes_per_warp]
+  int const_mech;           // 1: the packed table is in the constant bank
 };
 
 struct RoundsGrids {
@@ -156,5 +157,30 @@ rounds::RState rounds_carve(void* base, long long cap, int N, int lut_bytes);
 cudaError_t rounds_grids_for(int N, int lut_bytes, const RoundsSetupLayout& SL, int sm_count, RoundsGrids* G);
 cudaError_t rounds_launch(int N, int lut_bytes, int what, const RoundsParams& R, const RoundsGrids& G, int after_rhs,
                           cudaStream_t st);
+
+// ------------------------------------------- packed constant-memory table
+// The round integrator's right-hand side reads the mechanism from constant
+// memory (all lanes of a warp read the same reaction at the same time, which
+// the constant cache serves as one broadcast): one record per reaction plus
+// the species data.  Byte offsets are from the start of the blob.
+struct CMechHeader {
+  int N, R, n_eff, pad;
+  int off_nasa, off_mw, off_imw, off_rxn, off_effsp, off_effm1, bytes, pad2;
+};
+struct RxnC {
+  double lnA, b, ea;        // forward (high-pressure limit for falloff): ln A, b, Ea/R
+  double lnA0, b0, ea0;     // low-pressure limit (falloff)
+  double ta, t3i, t1i, t2;  // Troe: alpha, 1/T***, 1/T*, T**
+  double sdnu;              // net stoichiometric change
+  double lr, br, er;        // explicit reverse Arrhenius
+  signed char sp[8];        // slots: reactants 0..3, products 4..7 (-1 empty)
+  signed char nu[8];        // signed stoichiometry of each slot
+  short type, flags, e0, e1;  // kind, flag bits, third-body efficiency range
+};
+static_assert(sizeof(RxnC) == 136, "packed reaction record");
+constexpr int kConstMechBytes = 60 * 1024;
+
+// Upload a packed table to the round integrator's constant bank on `st`.
+cudaError_t rounds_upload_const(const void* blob, int bytes, cudaStream_t st);
 
 }  // namespace b200

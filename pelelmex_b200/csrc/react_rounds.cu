@@ -198,7 +198,132 @@ __device__ __forceinline__ void r_rhs(const DevMech& m, const RVec<NS + 1>& v, d
   v.fv(NS) = (v.F(NS) - hs) / rcp;
 }
 
+// ------------------------------------------------ constant-memory table
+__constant__ __align__(16) unsigned char c_mech[kConstMechBytes];
+
+__device__ __forceinline__ const CMechHeader& cm_hdr() { return *reinterpret_cast<const CMechHeader*>(c_mech); }
+__device__ __forceinline__ const double* cm_d(int off) { return reinterpret_cast<const double*>(c_mech + off); }
+
+// NASA-7 cp/R, h/RT, g/RT of species k at T from the constant table.
+__device__ __forceinline__ void cm_nasa7(const CMechHeader& H, int k, double T, double lnT, double invT,
+                                        double& cpR, double& hRT, double& gRT) {
+  const double* nasa = cm_d(H.off_nasa);
+  const int N = H.N;
+  const int base = (T < nasa[k]) ? 1 : 8;
+  const double a0 = nasa[(base + 0) * N + k], a1 = nasa[(base + 1) * N + k], a2 = nasa[(base + 2) * N + k];
+  const double a3 = nasa[(base + 3) * N + k], a4 = nasa[(base + 4) * N + k], a5 = nasa[(base + 5) * N + k];
+  const double a6 = nasa[(base + 6) * N + k];
+  cpR = a0 + T * (a1 + T * (a2 + T * (a3 + T * a4)));
+  hRT = a0 + T * (a1 / 2 + T * (a2 / 3 + T * (a3 / 4 + T * a4 / 5))) + a5 * invT;
+  const double sR = a0 * lnT + T * (a1 + T * (a2 / 2 + T * (a3 / 3 + T * a4 / 4))) + a6;
+  gRT = hRT - sR;
+}
+
+// Rate of progress of reaction j from the constant table (same formulas as
+// r_progress).
+__device__ __forceinline__ double cm_progress(const CMechHeader& H, int j, double T, double lnT, double invT,
+                                              double Ctot, double lnPRT, const double* sC, const double* sG,
+                                              int ss) {
+  const RxnC& r = reinterpret_cast<const RxnC*>(c_mech + H.off_rxn)[j];
+  const int type = r.type, flags = r.flags;
+  const double kinf = exp(r.lnA + r.b * lnT - r.ea * invT);
+  double M = 0.0;
+  if (type != 0) {
+    M = Ctot;
+    const short* esp = reinterpret_cast<const short*>(c_mech + H.off_effsp);
+    const double* em1 = cm_d(H.off_effm1);
+    for (int q = r.e0; q < r.e1; ++q) M += em1[q] * sC[esp[q] * ss];
+  }
+  double kf = kinf;
+  if (type >= 2) {
+    const double k0 = exp(r.lnA0 + r.b0 * lnT - r.ea0 * invT);
+    const double Pr = k0 * M / kinf;
+    double F = 1.0;
+    if (type == 3) {
+      double Fc = (1.0 - r.ta) * exp(-T * r.t3i) + r.ta * exp(-T * r.t1i);
+      if (flags & 4) Fc += exp(-r.t2 * invT);
+      const double logFc = log10(fmax(Fc, 1e-300));
+      const double c = -0.4 - 0.67 * logFc, nn = 0.75 - 1.27 * logFc;
+      const double u = log10(fmax(Pr, 1e-300)) + c;
+      const double f1 = u / (nn - 0.14 * u);
+      F = exp(kLn10 * (logFc / (1.0 + f1 * f1)));
+    }
+    kf = kinf * Pr / (1.0 + Pr) * F;
+  }
+  double pf = 1.0, pr = 1.0, sg = 0.0;
+#pragma unroll
+  for (int sl = 0; sl < 8; ++sl) {
+    const int k = r.sp[sl];
+    if (k >= 0) {
+      const int nu = r.nu[sl];
+      const int na = nu < 0 ? -nu : nu;
+      const double ck = sC[k * ss];
+      double p = ck;
+      for (int e = 1; e < na; ++e) p *= ck;
+      if (sl < 4) pf *= p;
+      else pr *= p;
+      sg += nu * sG[k * ss];
+    }
+  }
+  double kr = 0.0;
+  if (flags & 2) kr = exp(r.lr + r.br * lnT - r.er * invT);
+  else if (flags & 1) kr = kf * exp(sg - r.sdnu * lnPRT);
+  double q = kf * pf - kr * pr;
+  if (type == 1) q *= M;
+  return q;
+}
+
+// HP right-hand side from the constant table (thread per cell).
+template <int NS>
+__device__ __forceinline__ void cm_rhs(const RVec<NS + 1>& v, double* sC, double* sG, double* sW, int ss) {
+  const CMechHeader& H = cm_hdr();
+  const double* imw = cm_d(H.off_imw);
+  const double* mw = cm_d(H.off_mw);
+  const double T = v.yev(NS);
+  const double lnT = log(T), invT = 1.0 / T;
+  double Ctot = 0.0, rcp = 0.0;
+#pragma unroll 1
+  for (int k = 0; k < NS; ++k) {
+    double cpR, hRT, gRT;
+    cm_nasa7(H, k, T, lnT, invT, cpR, hRT, gRT);
+    const double yk = v.yev(k);
+    const double Ck = yk * imw[k];
+    sC[k * ss] = Ck;
+    sG[k * ss] = gRT;
+    sW[k * ss] = 0.0;
+    Ctot += Ck;
+    rcp += yk * cpR * kRu * imw[k];
+  }
+  const double lnPRT = log(kPatm / (kRu * T));
+  const int R = H.R;
+  const RxnC* rx = reinterpret_cast<const RxnC*>(c_mech + H.off_rxn);
+#pragma unroll 1
+  for (int j = 0; j < R; ++j) {
+    const double q = cm_progress(H, j, T, lnT, invT, Ctot, lnPRT, sC, sG, ss);
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+      const int k = rx[j].sp[sl];
+      if (k >= 0) sW[k * ss] += (double)rx[j].nu[sl] * q;
+    }
+  }
+  double hs = 0.0;
+#pragma unroll 1
+  for (int k = 0; k < NS; ++k) {
+    double cpR, hRT, gRT;
+    cm_nasa7(H, k, T, lnT, invT, cpR, hRT, gRT);
+    const double yd = sW[k * ss] * mw[k] + v.F(k);
+    v.fv(k) = yd;
+    hs += hRT * kRu * T * imw[k] * yd;
+  }
+  v.fv(NS) = (v.F(NS) - hs) / rcp;
+}
+
 }  // namespace
+
+cudaError_t rounds_upload_const(const void* blob, int bytes, cudaStream_t st) {
+  if (bytes > kConstMechBytes) return cudaErrorInvalidValue;
+  return cudaMemcpyToSymbolAsync(c_mech, blob, (size_t)bytes, 0, cudaMemcpyHostToDevice, st);
+}
 
 // ---------------------------------------------------------------- kernels
 template <int NS>
@@ -272,7 +397,8 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
     const int slot = R.list_in[idx];
     const RVec<n> v{reinterpret_cast<double*>(rec_of(R.S, slot) + R.S.L.off_vec)};
-    r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
+    if (R.const_mech) cm_rhs<NS>(v, sC, sG, sW, blockDim.x);
+    else r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
   }
 }
 
