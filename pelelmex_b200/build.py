@@ -42,21 +42,36 @@ def _stale(target: Path, deps) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+def write_generated(gendir: Path) -> Path:
+    """Mechanism-specific right-hand sides of the bundled mechanisms
+    (pelelmex_b200.mechgen); the file is rewritten only when it changes."""
+    sys.path.insert(0, str(ROOT))
+    from pelelmex_b200 import mechgen
+    gendir.mkdir(parents=True, exist_ok=True)
+    path = gendir / "gen_mechs.cuh"
+    text = mechgen.generate_bundled()
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+    return path
+
+
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False, jobs: int = 0) -> Path:
     """Compile every csrc/*.cu to an object in parallel, then link libb200chem.so."""
     import concurrent.futures as cf
     import os
 
-    deps = list(CSRC.glob("*")) + list(INCLUDE.rglob("*.h")) + list(INCLUDE.rglob("*.H"))
-    if not force and not _stale(LIB, deps):
-        return LIB
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
+    gen = write_generated(objdir / "gen")
+    deps = list(CSRC.glob("*")) + list(INCLUDE.rglob("*.h")) + list(INCLUDE.rglob("*.H")) + [gen]
+    if not force and not _stale(LIB, deps):
+        return LIB
     srcs = sources()
 
     def compile_one(src: Path):
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", "-o", str(obj), str(src), "-I", str(INCLUDE)]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", "-o", str(obj), str(src), "-I", str(INCLUDE), "-I",
+               str(gen.parent)]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
         return src, obj, cmd, subprocess.run(cmd, capture_output=True, text=True)

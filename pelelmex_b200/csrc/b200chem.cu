@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -211,6 +212,7 @@ struct b200chem_reactor {
   long long launches = 0;  // kernels launched by this handle (instrumentation)
   unsigned char* h_cmech = nullptr;  // pinned packed constant-memory table (null: too large)
   int cmech_bytes = 0;
+  int gen_mech = 0;  // 1: a generated right-hand side matches the mechanism
 };
 
 namespace b200 {
@@ -371,6 +373,7 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   R.wscratch = static_cast<unsigned char*>(h->d_rwarp);
   // the right-hand side reads the mechanism from the constant bank when it fits
   R.const_mech = h->cmech_bytes > 0 ? 1 : 0;
+  R.gen_mech = h->gen_mech && !getenv("B200CHEM_NO_GENERATED_RHS");
   if (R.const_mech) CK(rounds_upload_const(h->h_cmech, h->cmech_bytes, st));
   const long long max_rounds = 64LL * std::max(1, (int)h->opts.max_steps) + 1024;
   for (long long chunk0 = 0; chunk0 < P.total; chunk0 += cap) {
@@ -609,6 +612,33 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
     }
   }
   incptr[N] = (int)incrxn.size();
+  // mechanism digest (FNV-1a over the description arrays, as pelelmex_b200.mechgen)
+  {
+    unsigned long long hsh = 0xcbf29ce484222325ull;
+    auto fnv = [&](const void* p, size_t bytes) {
+      const unsigned char* c = static_cast<const unsigned char*>(p);
+      for (size_t i = 0; i < bytes; ++i) {
+        hsh ^= c[i];
+        hsh *= 0x100000001b3ull;
+      }
+    };
+    const int32_t hdr3[3] = {md->n_species, md->n_reactions, md->n_eff};
+    fnv(hdr3, sizeof(hdr3));
+    fnv(md->mw, sizeof(double) * N);
+    fnv(md->nasa, sizeof(double) * 15 * (size_t)N);
+    fnv(md->rtype, sizeof(int32_t) * R);
+    fnv(md->rflags, sizeof(int32_t) * R);
+    fnv(md->arr, sizeof(double) * 3 * (size_t)R);
+    fnv(md->arr_lo, sizeof(double) * 3 * (size_t)R);
+    fnv(md->arr_rev, sizeof(double) * 3 * (size_t)R);
+    fnv(md->troe, sizeof(double) * 4 * (size_t)R);
+    fnv(md->sp, sizeof(int32_t) * 8 * (size_t)R);
+    fnv(md->nu, sizeof(int32_t) * 8 * (size_t)R);
+    fnv(md->eff_ptr, sizeof(int32_t) * (R + 1));
+    fnv(md->eff_sp, sizeof(int32_t) * (size_t)md->n_eff);
+    fnv(md->eff_val, sizeof(double) * (size_t)md->n_eff);
+    h->gen_mech = (rounds_generated_for(hsh) == N) ? 1 : 0;
+  }
   // packed constant-memory table of the round integrator's right-hand side
   std::vector<unsigned char> cblob;
   {

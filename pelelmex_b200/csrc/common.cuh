@@ -136,6 +136,7 @@ struct RoundsParams {
   int* cnt_setup;
   unsigned char* wscratch;  // [setup warps][SL.gbytes_per_warp]
   int const_mech;           // 1: the packed table is in the constant bank
+  int gen_mech;             // 1: the mechanism has a generated right-hand side
 };
 
 struct RoundsGrids {
@@ -179,6 +180,10 @@ struct RxnC {
 };
 static_assert(sizeof(RxnC) == 136, "packed reaction record");
 constexpr int kConstMechBytes = 60 * 1024;
+
+// Species count of the generated right-hand side whose mechanism digest
+// matches (0: none).
+int rounds_generated_for(unsigned long long digest);
 
 // Upload a packed table to the round integrator's constant bank on `st`.
 cudaError_t rounds_upload_const(const void* blob, int bytes, cudaStream_t st);

@@ -17,6 +17,7 @@
 
 #include "bdf_rounds.cuh"
 #include "common.cuh"
+#include "gen_mechs.cuh"  // mechanism-specific right-hand sides (written by the build)
 
 namespace b200 {
 using namespace rounds;
@@ -397,8 +398,16 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
     const int slot = R.list_in[idx];
     const RVec<n> v{reinterpret_cast<double*>(rec_of(R.S, slot) + R.S.L.off_vec)};
-    if (R.const_mech) cm_rhs<NS>(v, sC, sG, sW, blockDim.x);
-    else r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
+    if (R.gen_mech) {
+      // generated code for this mechanism: every coefficient an immediate
+      if constexpr (NS == 9) gen::gen_rhs_synth_h2_9(&v.yev(0), &v.F(0), &v.fv(0));
+      else if constexpr (NS == 21) gen::gen_rhs_synth_ch4_21(&v.yev(0), &v.F(0), &v.fv(0));
+      else if constexpr (NS == 53) gen::gen_rhs_synth_c12_53(&v.yev(0), &v.F(0), &v.fv(0));
+    } else if (R.const_mech) {
+      cm_rhs<NS>(v, sC, sG, sW, blockDim.x);
+    } else {
+      r_rhs<NS>(s_mech, v, sC, sG, sW, blockDim.x);
+    }
   }
 }
 
@@ -909,4 +918,15 @@ cudaError_t rounds_launch(int N, int lut_bytes, int what, const RoundsParams& R,
   return cudaErrorInvalidValue;
 }
 
+}  // namespace b200
+
+namespace b200 {
+// Generated right-hand side matching a mechanism digest: 0 none, else the
+// species count of the generated code.
+int rounds_generated_for(unsigned long long digest) {
+  if (digest == gen::kGenDigest_synth_h2_9) return 9;
+  if (digest == gen::kGenDigest_synth_ch4_21) return 21;
+  if (digest == gen::kGenDigest_synth_c12_53) return 53;
+  return 0;
+}
 }  // namespace b200
