@@ -418,7 +418,10 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
 #endif
 
 // Lanes per cell of the control kernel.
-constexpr int ctrl_group(int n) { return n <= 32 ? 8 : 16; }
+#ifndef B200_CTRL_LANES
+#define B200_CTRL_LANES 8
+#endif
+constexpr int ctrl_group(int n) { return n <= 32 ? B200_CTRL_LANES : 16; }
 
 // Resume the cells of list_in, G lanes per cell.  after_rhs: each consumes
 // the f just evaluated (counted in nfe); otherwise they come back from a
