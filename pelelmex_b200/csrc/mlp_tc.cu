@@ -49,6 +49,7 @@ struct GemmArgs {
   int epi;
   int n_valid;         // columns of C actually written (<= N)
   int* err;            // raised on an mbarrier timeout
+  int vec_ok;          // C (and aux) rows 16-byte aligned: vector epilogue
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -171,16 +172,23 @@ __device__ __forceinline__ void stage_tile(unsigned char* dst, const __nv_bfloat
   }
 }
 
+// hardware tanh approximation (MUFU); ample for BF16 activations
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ float gelu(float x) {
   // tanh form of GELU (Hendrycks & Gimpel 2016)
   const float k0 = 0.7978845608028654f, k1 = 0.044715f;
-  return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
+  return 0.5f * x * (1.0f + tanh_fast(k0 * (x + k1 * x * x * x)));
 }
 
 __device__ __forceinline__ float gelu_grad(float x) {
   const float k0 = 0.7978845608028654f, k1 = 0.044715f;
   const float u = k0 * (x + k1 * x * x * x);
-  const float t = tanhf(u);
+  const float t = tanh_fast(u);
   const float du = k0 * (1.0f + 3.0f * k1 * x * x);
   return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
 }
@@ -252,29 +260,66 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_bf16_tc(GemmArgs g) {
         const int col = col0 + i;
         if (col < g.n_valid && g.bias) v[i] += __ldg(g.bias + col);
       }
+      // full 32-column chunk with 16-byte aligned rows: vector loads / stores
+      const bool full = (col0 + 32 <= g.n_valid) && g.vec_ok;
       if (g.epi == kEpiF32) {
-        float* C = reinterpret_cast<float*>(g.C) + (long long)row * g.ldc;
+        float* C = reinterpret_cast<float*>(g.C) + (long long)row * g.ldc + col0;
+        if (full) {
 #pragma unroll
-        for (int i = 0; i < 32; ++i)
-          if (col0 + i < g.n_valid) C[col0 + i] = v[i];
-      } else {
-        __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (long long)row * g.ldc;
-        if (g.epi == kEpiGeluBf16) {
-          float* P = g.aux ? g.aux + (long long)row * g.ldc : nullptr;
-#pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            if (P && col0 + i < g.n_valid) P[col0 + i] = v[i];
-            v[i] = gelu(v[i]);
-          }
-        } else if (g.epi == kEpiDGeluBf16) {
-          const float* P = g.aux + (long long)row * g.ldc;
+          for (int q = 0; q < 8; ++q)
+            reinterpret_cast<float4*>(C)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
 #pragma unroll
           for (int i = 0; i < 32; ++i)
-            if (col0 + i < g.n_valid) v[i] *= gelu_grad(P[col0 + i]);
+            if (col0 + i < g.n_valid) C[i] = v[i];
         }
+      } else {
+        __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (long long)row * g.ldc + col0;
+        if (g.epi == kEpiGeluBf16) {
+          float* P = g.aux ? g.aux + (long long)row * g.ldc + col0 : nullptr;
+          if (P && full) {
 #pragma unroll
-        for (int i = 0; i < 32; ++i)
-          if (col0 + i < g.n_valid) C[col0 + i] = __float2bfloat16_rn(v[i]);
+            for (int q = 0; q < 8; ++q)
+              reinterpret_cast<float4*>(P)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          } else if (P) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+              if (col0 + i < g.n_valid) P[i] = v[i];
+          }
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] = gelu(v[i]);
+        } else if (g.epi == kEpiDGeluBf16) {
+          const float* P = g.aux + (long long)row * g.ldc + col0;
+          if (full) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float4 p = reinterpret_cast<const float4*>(P)[q];
+              v[4 * q] *= gelu_grad(p.x);
+              v[4 * q + 1] *= gelu_grad(p.y);
+              v[4 * q + 2] *= gelu_grad(p.z);
+              v[4 * q + 3] *= gelu_grad(p.w);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+              if (col0 + i < g.n_valid) v[i] *= gelu_grad(P[i]);
+          }
+        }
+        if (full) {
+          uint32_t w[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+            w[q] = *reinterpret_cast<const uint32_t*>(&b2);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            reinterpret_cast<uint4*>(C)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (col0 + i < g.n_valid) C[i] = __float2bfloat16_rn(v[i]);
+        }
       }
     }
     // all warps have read the accumulator before the next tile overwrites it
@@ -318,6 +363,12 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
   g.epi = epi;
   g.n_valid = n_valid > 0 ? n_valid : N;
   g.err = err;
+  {
+    const size_t esz = (epi == kEpiF32) ? 4 : 2;
+    const bool cal = (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ((ldc * (long long)esz) & 15) == 0;
+    const bool aal = !aux || ((reinterpret_cast<uintptr_t>(aux) & 15) == 0 && ((ldc * 4) & 15) == 0);
+    g.vec_ok = (cal && aal) ? 1 : 0;
+  }
   const bool resident = (K <= 256 && N <= 256);
   const int NT = N <= 256 ? N : 256;
   const int KC = resident ? K : 64;
