@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--cells", type=int, default=0,
                    help="react only this many seeded random cells of the field (small profiling cases)")
     p.add_argument("--no-hybrid", action="store_true", help="plain BDF only (no surrogate arm)")
+    p.add_argument("--no-autotune", action="store_true", help="default launch shape (no autotuner pass)")
+    p.add_argument("--tune-cells", type=int, default=262144, help="cells of the autotuner's sample")
     p.add_argument("--train-cells", type=int, default=524288, help="BDF-labelled training cells of the surrogate")
     p.add_argument("--train-steps", type=int, default=3000, help="optimizer steps per ensemble member")
     return p.parse_args()
@@ -252,6 +254,20 @@ def run_b200(args, rank, world, local_rank):
     def barrier():
         if world > 1:
             dist.barrier()
+
+    # launch shape: the autotuner times react on a seeded sample of the same
+    # field distribution (untimed, before the warm-up)
+    if not args.no_autotune:
+        tf = sample_field(mech, args, min(args.tune_cells, nc), seed=77)
+        td = {k: torch.tensor(getattr(tf, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
+        t0 = time.perf_counter()
+        tuning, tune_ms = r.autotune(td["rhoY"], td["frhoY"], td["T"], td["rhoH"], td["frhoH"], field.dt,
+                                     max_trials=32)
+        cfg["launch_tuning"] = dict(tuning, sample_cells=tf.ncells, sample_ms=round(tune_ms, 3),
+                                    seconds=round(time.perf_counter() - t0, 2))
+        del td
+    else:
+        cfg["launch_tuning"] = dict(r.get_tuning(), autotuned=False)
 
     # warm-up; the first call also collects the integrator's counters
     counters = None

@@ -203,6 +203,42 @@ int b200chem_destroy(b200chem_handle h);
  * reference counterpart).  -1 for a NULL handle. */
 int64_t b200chem_kernel_launches(b200chem_handle h);
 
+/* ------------------------------------------------------- launch tuning
+ * Launch shape of the round-based integrator (opts.kernel 0 or 3).  No
+ * reference counterpart: the reference's GPU reactors fix their launch
+ * shape at compile time.  Zero fields take the defaults. */
+typedef struct b200chem_tuning {
+  int32_t rhs_ctas_per_sm;   /* CTAs per SM of the right-hand-side kernel (0: as many as fit) */
+  int32_t ctrl_ctas_per_sm;  /* ... of the step-control / Newton kernel                      */
+  int32_t jac_ctas_per_sm;   /* ... of the Jacobian kernel                                   */
+  int32_t gj_ctas_per_sm;    /* ... of the iteration-matrix inversion kernel                 */
+  int32_t rounds_per_check;  /* rounds between two reads of the live-cell count: 2, 4, 8
+                                or 16 (0: 4)                                                 */
+  int32_t use_graph;         /* 1: the rounds between two checks are replayed from one
+                                captured CUDA graph; 2: launched one by one (0: 1)          */
+  int32_t rhs_form;          /* 0: generated mechanism code when it matches, else the
+                                constant bank, else global tables; 1: constant bank (or
+                                global tables); 2: global tables                             */
+  int32_t reserved;
+} b200chem_tuning;
+
+/* Current launch shape (the defaults until set). */
+int b200chem_get_tuning(b200chem_handle h, b200chem_tuning* t);
+/* Sets the launch shape used by later react calls; B200CHEM_EINVAL for
+ * values outside the ranges above. */
+int b200chem_set_tuning(b200chem_handle h, const b200chem_tuning* t);
+
+/* Autotuner: times react on a copy of the given cells (flat layout of
+ * b200chem_react_flat, at most 2^20 cells are used; the inputs are NOT
+ * modified) under candidate launch shapes, by coordinate descent over the
+ * fields of b200chem_tuning, keeps the fastest shape in the handle and
+ * returns it in best (may be NULL).  *best_ms receives the time of one react
+ * call of the sample under that shape (may be NULL).  max_trials bounds the
+ * number of timed react calls (0: 48). */
+int b200chem_autotune(b200chem_handle h, const double* rhoY, const double* extF_rhoY, const double* T,
+                      const double* rhoH, const double* extF_rhoH, int64_t ncells, double dt_react,
+                      int32_t max_trials, void* stream, b200chem_tuning* best, double* best_ms);
+
 const char* b200chem_last_error(void);
 int b200chem_version(void);
 

@@ -50,6 +50,13 @@ class GateOpts(ctypes.Structure):
                 ("dT_max", ctypes.c_double), ("t_source", ctypes.c_int32), ("residual_t_only", ctypes.c_int32)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("rhs_ctas_per_sm", ctypes.c_int32), ("ctrl_ctas_per_sm", ctypes.c_int32),
+                ("jac_ctas_per_sm", ctypes.c_int32), ("gj_ctas_per_sm", ctypes.c_int32),
+                ("rounds_per_check", ctypes.c_int32), ("use_graph", ctypes.c_int32), ("rhs_form", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class B200ChemError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"b200chem error {code}: {msg}")
@@ -98,6 +105,13 @@ def load(path: os.PathLike | None = None):
     L.b200chem_surrogate_gate.restype = ctypes.c_int
     L.b200chem_kernel_launches.argtypes = [ctypes.c_void_p]
     L.b200chem_kernel_launches.restype = ctypes.c_int64
+    L.b200chem_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+    L.b200chem_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+    L.b200chem_autotune.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int64,
+                                    ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Tuning),
+                                    ctypes.POINTER(ctypes.c_double)]
+    for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):
         f = getattr(L, name)
         f.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, _f64p, ctypes.c_void_p]

@@ -213,6 +213,10 @@ struct b200chem_reactor {
   unsigned char* h_cmech = nullptr;  // pinned packed constant-memory table (null: too large)
   int cmech_bytes = 0;
   int gen_mech = 0;  // 1: a generated right-hand side matches the mechanism
+  b200chem_tuning tune{};           // launch shape of the round-based integrator
+  cudaStream_t cap_stream = nullptr;  // private stream the round graph is captured on
+  cudaGraphExec_t rgraph = nullptr;   // executable graph of rounds_per_check rounds
+  int rgraph_rounds = 0;              // rounds in rgraph
 };
 
 namespace b200 {
@@ -304,7 +308,7 @@ int launch_thread_per_cell(b200chem_reactor* h, const ReactParams& P, cudaStream
 
 // Cell-state budget of one chunk of the round-based integrator.
 constexpr long long kRoundsBudgetBytes = 24LL << 30;
-// Rounds between checks of the live-cell count (one host sync each).
+// Default rounds between checks of the live-cell count (one host sync each).
 constexpr int kRoundsCheckEvery = 4;
 
 int ensure_buffer(void** p, size_t* have, size_t bytes, cudaStream_t st, const char* what) {
@@ -324,6 +328,103 @@ int ensure_buffer(void** p, size_t* have, size_t bytes, cudaStream_t st, const c
   return 0;
 }
 
+int tuning_valid(const b200chem_tuning& t) {
+  const int32_t per_sm[4] = {t.rhs_ctas_per_sm, t.ctrl_ctas_per_sm, t.jac_ctas_per_sm, t.gj_ctas_per_sm};
+  for (int32_t v : per_sm)
+    if (v < 0 || v > 64) return 0;
+  if (t.rounds_per_check != 0 && t.rounds_per_check != 2 && t.rounds_per_check != 4 && t.rounds_per_check != 8 &&
+      t.rounds_per_check != 16)
+    return 0;
+  if (t.use_graph < 0 || t.use_graph > 2) return 0;
+  if (t.rhs_form < 0 || t.rhs_form > 2) return 0;
+  return 1;
+}
+
+int32_t& tuning_field(b200chem_tuning& t, int field) {
+  switch (field) {
+    case 0: return t.rhs_ctas_per_sm;
+    case 1: return t.ctrl_ctas_per_sm;
+    case 2: return t.jac_ctas_per_sm;
+    case 3: return t.gj_ctas_per_sm;
+    case 4: return t.rounds_per_check;
+    case 5: return t.use_graph;
+    default: return t.rhs_form;
+  }
+}
+
+// Grid of one kernel: the occupancy maximum, capped by the tuned CTAs per SM.
+int tuned_grid(int max_grid, int sm_count, int per_sm) {
+  if (per_sm <= 0) return max_grid;
+  return std::max(sm_count, std::min(max_grid, per_sm * sm_count));
+}
+
+// One round of the integrator: right-hand sides of the cells in list_in,
+// step control (Newton update, error test, next prediction) appending to
+// list_out and to the setup list, Jacobian and iteration-matrix inversion of
+// the setup list, step control of the cells back from their setup.
+int enqueue_round(b200chem_reactor* h, int lut, RoundsParams R, const RoundsGrids& G, int* list_in, int* cnt_in,
+                  int* list_out, int* cnt_out, int* list_setup, int* cnt_setup, cudaStream_t st) {
+  R.list_in = list_in;
+  R.cnt_in = cnt_in;
+  R.list_out = list_out;
+  R.cnt_out = cnt_out;
+  R.list_setup = list_setup;
+  R.cnt_setup = cnt_setup;
+  CK(rounds_launch(h->N, lut, kRoundsRhs, R, G, 0, st));
+  CK(cudaMemsetAsync(cnt_out, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(cnt_setup, 0, sizeof(int), st));
+  CK(rounds_launch(h->N, lut, kRoundsCtrl, R, G, 1, st));
+  R.list_in = list_setup;
+  R.cnt_in = cnt_setup;
+  CK(rounds_launch(h->N, lut, kRoundsJac, R, G, 0, st));
+  CK(rounds_launch(h->N, lut, kRoundsGj, R, G, 0, st));
+  // cells coming back from a setup always ask for a right-hand side next
+  CK(rounds_launch(h->N, lut, kRoundsCtrl, R, G, 0, st));
+  return 0;
+}
+
+// Captures `rounds` rounds (an even number: the two slot lists swap roles
+// every round, so the graph starts and ends on list A) into h->rgraph,
+// updating the executable graph in place when only kernel parameters
+// changed.
+int capture_rounds(b200chem_reactor* h, int lut, const RoundsParams& R, const RoundsGrids& G, int rounds, int* lst[2],
+                   int* cnt[2], int* listS, int* cntS) {
+  if (!h->cap_stream) CK(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+  CK(cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int err = 0;
+  for (int r = 0; r < rounds && !err; ++r) {
+    const int cur = r & 1;
+    err = enqueue_round(h, lut, R, G, lst[cur], cnt[cur], lst[1 - cur], cnt[1 - cur], listS, cntS, h->cap_stream);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->cap_stream, &g);
+  if (err || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return err ? err : set_err(B200CHEM_ECUDA, "graph capture of the rounds failed: %s", cudaGetErrorString(ce));
+  }
+  if (h->rgraph && h->rgraph_rounds == rounds) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(h->rgraph, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(h->rgraph);
+      h->rgraph = nullptr;
+    }
+  } else if (h->rgraph) {
+    cudaGraphExecDestroy(h->rgraph);
+    h->rgraph = nullptr;
+  }
+  cudaError_t ie = cudaSuccess;
+  if (!h->rgraph) ie = cudaGraphInstantiate(&h->rgraph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    h->rgraph = nullptr;
+    return set_err(B200CHEM_ECUDA, "cannot instantiate the round graph: %s", cudaGetErrorString(ie));
+  }
+  h->rgraph_rounds = rounds;
+  return 0;
+}
+
 // Round-based integrator: rhs / ctrl / setup kernels over compacted lists,
 // chunk by chunk (see react_rounds.cu).
 int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
@@ -338,6 +439,14 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     CK(rounds_grids_for(h->N, lut, SL, h->sm_count, &h->rgrid));
     h->rgrid_lut = lut;
   }
+  const b200chem_tuning& T = h->tune;
+  RoundsGrids G = h->rgrid;
+  G.rhs = tuned_grid(h->rgrid.rhs, h->sm_count, T.rhs_ctas_per_sm);
+  G.ctrl = tuned_grid(h->rgrid.ctrl, h->sm_count, T.ctrl_ctas_per_sm);
+  G.jac = tuned_grid(h->rgrid.jac, h->sm_count, T.jac_ctas_per_sm);
+  G.gj = tuned_grid(h->rgrid.gj, h->sm_count, T.gj_ctas_per_sm);
+  const int per_check = T.rounds_per_check > 0 ? T.rounds_per_check : kRoundsCheckEvery;
+  const bool graph = T.use_graph != 2;
   // chunk capacity from the state budget (and the free device memory)
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
@@ -364,16 +473,15 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   if (rec_bytes + 12ull * cap > h->rounds_bytes)
     return set_err(B200CHEM_ECUDA, "round-integrator state layout overflows its buffer");
   int* lists = reinterpret_cast<int*>(static_cast<unsigned char*>(h->d_rounds) + rec_bytes);
-  int* listA = lists;
-  int* listB = lists + cap;
+  int* lst[2] = {lists, lists + cap};
   int* listS = lists + 2 * cap;
-  int* cntA = h->d_rcnt;
-  int* cntB = h->d_rcnt + 1;
+  int* cnt[2] = {h->d_rcnt, h->d_rcnt + 1};
   int* cntS = h->d_rcnt + 2;
   R.wscratch = static_cast<unsigned char*>(h->d_rwarp);
-  // the right-hand side reads the mechanism from the constant bank when it fits
-  R.const_mech = h->cmech_bytes > 0 ? 1 : 0;
-  R.gen_mech = h->gen_mech && !getenv("B200CHEM_NO_GENERATED_RHS");
+  // right-hand-side form: generated mechanism code, the constant bank or the
+  // global tables
+  R.const_mech = (h->cmech_bytes > 0 && T.rhs_form <= 1) ? 1 : 0;
+  R.gen_mech = (h->gen_mech && T.rhs_form == 0) ? 1 : 0;
   if (R.const_mech) CK(rounds_upload_const(h->h_cmech, h->cmech_bytes, st));
   const long long max_rounds = 64LL * std::max(1, (int)h->opts.max_steps) + 1024;
   for (long long chunk0 = 0; chunk0 < P.total; chunk0 += cap) {
@@ -382,44 +490,32 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     CK(cudaMemsetAsync(h->d_rcnt, 0, 4 * sizeof(int), st));
     R.list_in = nullptr;
     R.cnt_in = nullptr;
-    R.list_out = listA;
-    R.cnt_out = cntA;
+    R.list_out = lst[0];
+    R.cnt_out = cnt[0];
     R.list_setup = listS;
     R.cnt_setup = cntS;
-    CK(rounds_launch(h->N, lut, kRoundsStart, R, h->rgrid, 0, st));
-      h->launches++;
-    int* lst[2] = {listA, listB};
-    int* cnt[2] = {cntA, cntB};
-    int cur = 0;
-    for (long long round = 0;; ++round) {
+    CK(rounds_launch(h->N, lut, kRoundsStart, R, G, 0, st));
+    h->launches++;
+    if (graph) {
+      err = capture_rounds(h, lut, R, G, per_check, lst, cnt, listS, cntS);
+      if (err) return err;
+    }
+    for (long long round = 0;; round += per_check) {
       if (round >= max_rounds) return set_err(B200CHEM_EINTEGRATE, "round-based integrator did not finish");
-      R.list_in = lst[cur];
-      R.cnt_in = cnt[cur];
-      R.list_out = lst[1 - cur];
-      R.cnt_out = cnt[1 - cur];
-      R.list_setup = listS;
-      R.cnt_setup = cntS;
-      CK(rounds_launch(h->N, lut, kRoundsRhs, R, h->rgrid, 0, st));
-      h->launches++;
-      CK(cudaMemsetAsync(cnt[1 - cur], 0, sizeof(int), st));
-      CK(cudaMemsetAsync(cntS, 0, sizeof(int), st));
-      CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 1, st));
-      h->launches++;
-      R.list_in = listS;
-      R.cnt_in = cntS;
-      CK(rounds_launch(h->N, lut, kRoundsJac, R, h->rgrid, 0, st));
-      h->launches++;
-      CK(rounds_launch(h->N, lut, kRoundsGj, R, h->rgrid, 0, st));
-      h->launches++;
-      // cells coming back from a setup always ask for a right-hand side next
-      CK(rounds_launch(h->N, lut, kRoundsCtrl, R, h->rgrid, 0, st));
-      h->launches++;
-      cur = 1 - cur;
-      if ((round + 1) % kRoundsCheckEvery == 0) {
-        CK(cudaMemcpyAsync(h->h_rcnt, cnt[cur], sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (*h->h_rcnt == 0) break;
+      if (graph) {
+        CK(cudaGraphLaunch(h->rgraph, st));
+      } else {
+        for (int r = 0; r < per_check; ++r) {
+          const int cur = r & 1;
+          err = enqueue_round(h, lut, R, G, lst[cur], cnt[cur], lst[1 - cur], cnt[1 - cur], listS, cntS, st);
+          if (err) return err;
+        }
       }
+      h->launches += 5LL * per_check;
+      // per_check is even: the live cells are back in list A
+      CK(cudaMemcpyAsync(h->h_rcnt, cnt[0], sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (*h->h_rcnt == 0) break;
     }
   }
   return 0;
@@ -997,6 +1093,157 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
 
 int64_t b200chem_kernel_launches(b200chem_handle h) { return h ? h->launches : -1; }
 
+int b200chem_get_tuning(b200chem_handle h, b200chem_tuning* t) {
+  if (!h || !t) return set_err(B200CHEM_EINVAL, "bad arguments");
+  *t = h->tune;
+  return 0;
+}
+
+int b200chem_set_tuning(b200chem_handle h, const b200chem_tuning* t) {
+  if (!h || !t) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!tuning_valid(*t)) return set_err(B200CHEM_EINVAL, "tuning field out of range");
+  h->tune = *t;
+  return 0;
+}
+
+// Autotuner of the round-based integrator's launch shape.  Each trial copies
+// the sample into work arrays, runs one react over them between two events
+// and reads the elapsed time; coordinate descent over the tuning fields keeps
+// a value when it is at least 1% faster than the best so far.
+int b200chem_autotune(b200chem_handle h, const double* rhoY, const double* extF_rhoY, const double* T,
+                      const double* rhoH, const double* extF_rhoH, int64_t ncells, double dt_react,
+                      int32_t max_trials, void* stream, b200chem_tuning* best, double* best_ms) {
+  if (!h || ncells <= 0 || !rhoY || !extF_rhoY || !T || !rhoH || !extF_rhoH)
+    return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!(dt_react > 0.0)) return set_err(B200CHEM_EINVAL, "dt_react must be positive");
+  const int kern = (h->opts.kernel == 0) ? (rounds_supported(h->N) ? 3 : 2) : h->opts.kernel;
+  if (kern != 3) return set_err(B200CHEM_EINVAL, "the autotuner tunes the round-based integrator (kernel 0 or 3)");
+  if (max_trials <= 0) max_trials = 48;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int N = h->N;
+  const long long n = std::min<long long>(ncells, 1LL << 20);
+  // sample arrays: inputs (compact copies) then the work copies react updates
+  const size_t nb = sizeof(double) * (size_t)n;
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, nb * (2 * (size_t)N + 6 + (size_t)N + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(B200CHEM_ENOMEM, "cannot allocate the autotuner sample");
+  }
+  double* s_rhoY = buf;
+  double* s_T = s_rhoY + (size_t)N * n;
+  double* s_rhoH = s_T + n;
+  double* w_rhoY = s_rhoH + n;
+  double* w_T = w_rhoY + (size_t)N * n;
+  double* w_rhoH = w_T + n;
+  double* w_fct = w_rhoH + n;
+  double* s_fY = w_fct + n;
+  double* s_fH = s_fY + (size_t)N * n;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int err = 0;
+  auto cleanup = [&]() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(buf);
+  };
+  auto ck = [&](cudaError_t e) {
+    if (e != cudaSuccess && !err) err = set_err(B200CHEM_ECUDA, "CUDA error in the autotuner: %s", cudaGetErrorString(e));
+    return err;
+  };
+  const size_t src_pitch = sizeof(double) * (size_t)ncells;
+  if (ck(cudaMemcpy2DAsync(s_rhoY, nb, rhoY, src_pitch, nb, N, cudaMemcpyDeviceToDevice, st)) ||
+      ck(cudaMemcpy2DAsync(s_fY, nb, extF_rhoY, src_pitch, nb, N, cudaMemcpyDeviceToDevice, st)) ||
+      ck(cudaMemcpyAsync(s_T, T, nb, cudaMemcpyDeviceToDevice, st)) ||
+      ck(cudaMemcpyAsync(s_rhoH, rhoH, nb, cudaMemcpyDeviceToDevice, st)) ||
+      ck(cudaMemcpyAsync(s_fH, extF_rhoH, nb, cudaMemcpyDeviceToDevice, st)) || ck(cudaEventCreate(&e0)) ||
+      ck(cudaEventCreate(&e1))) {
+    cleanup();
+    return err;
+  }
+  const b200chem_tuning saved = h->tune;
+  int trials = 0;
+  // one timed react of the sample under tuning t; +inf when the shape fails
+  auto trial = [&](const b200chem_tuning& t, double* ms) -> int {
+    *ms = 1e300;
+    h->tune = t;
+    if (ck(cudaMemcpyAsync(w_rhoY, s_rhoY, nb * N, cudaMemcpyDeviceToDevice, st)) ||
+        ck(cudaMemcpyAsync(w_T, s_T, nb, cudaMemcpyDeviceToDevice, st)) ||
+        ck(cudaMemcpyAsync(w_rhoH, s_rhoH, nb, cudaMemcpyDeviceToDevice, st)) ||
+        ck(cudaMemsetAsync(w_fct, 0, nb, st)) || ck(cudaEventRecord(e0, st)))
+      return err;
+    double dt = dt_react;
+    const int rc = b200chem_react_flat(h, w_rhoY, s_fY, w_T, w_rhoH, s_fH, w_fct, nullptr, n, &dt, nullptr, st,
+                                       nullptr, nullptr);
+    ++trials;
+    if (ck(cudaEventRecord(e1, st)) || ck(cudaEventSynchronize(e1))) return err;
+    if (rc != 0) return 0;  // shape rejected: stays at +inf
+    float f = 0.f;
+    if (ck(cudaEventElapsedTime(&f, e0, e1))) return err;
+    *ms = f;
+    return 0;
+  };
+  b200chem_tuning cur = saved;
+  double cur_ms = 1e300, m = 0;
+  // warm-up (allocations, graph instantiation), then the starting point
+  if (trial(cur, &m) || trial(cur, &cur_ms)) {
+    h->tune = saved;
+    cleanup();
+    return err;
+  }
+  if (!(cur_ms < 1e300)) {
+    h->tune = saved;
+    cleanup();
+    return set_err(B200CHEM_EINTEGRATE, "react of the autotuner sample failed under the starting launch shape");
+  }
+  const int sm = h->sm_count;
+  const int max_per_sm[4] = {std::max(1, h->rgrid.rhs / sm), std::max(1, h->rgrid.ctrl / sm),
+                             std::max(1, h->rgrid.jac / sm), std::max(1, h->rgrid.gj / sm)};
+  for (int pass = 0; pass < 2 && !err && trials < max_trials; ++pass) {
+    for (int field = 0; field < 7 && !err && trials < max_trials; ++field) {
+      std::vector<int32_t> cand;
+      if (field < 4) {
+        cand.push_back(0);
+        for (int v = 1; v < max_per_sm[field]; v *= 2) cand.push_back(v);
+      } else if (field == 4) {
+        cand = {2, 4, 8, 16};
+      } else if (field == 5) {
+        cand = {1, 2};
+      } else {
+        if (h->gen_mech) cand.push_back(0);
+        if (h->cmech_bytes > 0) cand.push_back(1);
+        cand.push_back(2);
+      }
+      // the value the current shape effectively uses for this field
+      int32_t now = tuning_field(cur, field);
+      if (field == 4 && now == 0) now = kRoundsCheckEvery;
+      if (field == 5 && now == 0) now = 1;
+      if (field == 6 && now == 0 && !h->gen_mech) now = h->cmech_bytes > 0 ? 1 : 2;
+      if (field == 6 && now == 1 && h->cmech_bytes == 0) now = 2;
+      for (int32_t v : cand) {
+        if (v == now || trials >= max_trials) continue;
+        b200chem_tuning t = cur;
+        tuning_field(t, field) = v;
+        double ms = 0;
+        if (trial(t, &ms)) break;
+        if (ms < 0.99 * cur_ms) {
+          cur = t;
+          cur_ms = ms;
+          now = v;
+        }
+      }
+    }
+  }
+  if (err) {
+    h->tune = saved;
+    cleanup();
+    return err;
+  }
+  h->tune = cur;
+  if (best) *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  cleanup();
+  return 0;
+}
+
 
 int b200chem_destroy(b200chem_handle h) {
   if (!h) return 0;
@@ -1013,6 +1260,8 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->d_rcnt) cudaFree(h->d_rcnt);
   if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
   if (h->h_cmech) cudaFreeHost(h->h_cmech);
+  if (h->rgraph) cudaGraphExecDestroy(h->rgraph);
+  if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   delete h;
   return 0;
 }

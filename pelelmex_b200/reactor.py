@@ -171,6 +171,44 @@ class ReactorB200:
         self._need()
         return int(_lib.load().b200chem_kernel_launches(self._h))
 
+    TUNING_FIELDS = ("rhs_ctas_per_sm", "ctrl_ctas_per_sm", "jac_ctas_per_sm", "gj_ctas_per_sm",
+                     "rounds_per_check", "use_graph", "rhs_form")
+
+    def get_tuning(self) -> dict:
+        """Launch shape of the round-based integrator (b200chem_tuning)."""
+        self._need()
+        t = _lib.Tuning()
+        _lib.check(_lib.load().b200chem_get_tuning(self._h, ctypes.byref(t)))
+        return {f: int(getattr(t, f)) for f in self.TUNING_FIELDS}
+
+    def set_tuning(self, **fields):
+        """Sets fields of the launch shape (the others keep their values)."""
+        self._need()
+        cur = self.get_tuning()
+        for k, v in fields.items():
+            if k not in cur:
+                raise ValueError(f"unknown tuning field {k}")
+            cur[k] = int(v)
+        t = _lib.Tuning(**cur)
+        _lib.check(_lib.load().b200chem_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, rhoY, extF_rhoY, T, rhoH, extF_rhoH, dt_react, max_trials=0, stream=None):
+        """Times react on a copy of the given flat-layout cells under candidate
+        launch shapes and keeps the fastest; returns (tuning dict, ms of one
+        react of the sample).  The inputs are not modified."""
+        self._need()
+        torch = _torch()
+        nc = T.shape[0]
+        for t in (rhoY, extF_rhoY, T, rhoH, extF_rhoH):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("autotune needs contiguous float64 CUDA tensors")
+        best = _lib.Tuning()
+        ms = ctypes.c_double(0.0)
+        _lib.check(_lib.load().b200chem_autotune(
+            self._h, rhoY.data_ptr(), extF_rhoY.data_ptr(), T.data_ptr(), rhoH.data_ptr(), extF_rhoH.data_ptr(), nc,
+            float(dt_react), int(max_trials), _stream_ptr(stream), ctypes.byref(best), ctypes.byref(ms)))
+        return {f: int(getattr(best, f)) for f in self.TUNING_FIELDS}, float(ms.value)
+
     def close(self):
         if self._h:
             _lib.load().b200chem_destroy(self._h)
