@@ -423,6 +423,20 @@ __global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
 #endif
 constexpr int ctrl_group(int n) { return n <= 32 ? B200_CTRL_LANES : 16; }
 
+// L2 prefetch of the control kernel: 0 none; 1 the vectors and matrices of
+// each cell as it starts (they stream in while the step-control scalars are
+// processed); 2 also the scalars and vectors of the cell the group takes
+// next.
+#ifndef B200_CTRL_PREFETCH
+#define B200_CTRL_PREFETCH 1
+#endif
+
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16; a
+// hint: no completion to wait for).
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Resume the cells of list_in, G lanes per cell.  after_rhs: each consumes
 // the f just evaluated (counted in nfe); otherwise they come back from a
 // setup.
@@ -445,6 +459,10 @@ __global__ void __launch_bounds__(128, B200_CTRL_MIN_CTAS) rk_ctrl(RoundsParams 
     if (live) {
       slot = R.list_in[idx];
       unsigned char* rec = rec_of(R.S, slot);
+      if (B200_CTRL_PREFETCH >= 1 && gl == 0)
+        l2_prefetch(rec + R.S.L.off_vec, (uint32_t)(R.S.L.stride - R.S.L.off_vec));
+      if (B200_CTRL_PREFETCH >= 2 && gl == 0 && idx + nw * GPW < cnt)
+        l2_prefetch(rec_of(R.S, R.list_in[idx + nw * GPW]), (uint32_t)R.S.L.off_j);
       load_cell(c, rec);
       if (after_rhs) c.cnt.nfe++;
       const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
