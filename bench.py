@@ -48,7 +48,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--edge", type=int, default=128)
-    p.add_argument("--dt", type=float, default=1e-6)
+    p.add_argument("--dt", type=float, default=None,
+                   help="dt_react (default 1e-6 s; 5e-6 s for the dodecane random field)")
+    p.add_argument("--workload", default="flame_ch4", choices=["flame_ch4", "c12_boxes", "c12_grf"],
+                   help="flame_ch4: drm19-shaped 128^3 flame field (the headline); c12_boxes: dodecane AMR-like "
+                        "list of 40 boxes in one launch; c12_grf: dodecane random-field flame at --edge^3")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -459,12 +463,179 @@ def run_b200(args, rank, world, local_rank):
     r.close()
 
 
+# ------------------------------------------------------ dodecane workloads
+C12 = "synth_c12_53"
+
+
+def run_dodecane(args, rank, world, local_rank):
+    """The dodecane workloads (53 species + T): the AMR-like box list (all of
+    this rank's boxes in one react launch, boxes dealt round-robin over the
+    ranks) or the random-field flame (flat, cells split over the ranks).
+    Same timing rules as the headline line; the CPU baseline is the oracle
+    on a bounded seeded sample of the same cells."""
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    mech = mechmod.builtin(C12)
+    N = mech.n_species
+    if args.workload == "c12_boxes":
+        boxes = workloads.c12_boxes(mech, dt=args.dt)
+        mine = boxes[rank::world]
+        total = sum(f.ncells for _, _, f in boxes)
+        wl = (f"c12_boxes: {len(boxes)} dodecane boxes (edges 16/32/64, half cold 300-600 K, half igniting "
+              f"900-1400 K, phi 0.5-2), {total} cells, one react launch per box list")
+        flat = [f for _, _, f in mine]
+    else:
+        n_all = args.edge ** 3
+        idx = np.arange(rank, n_all, world, dtype=np.int64)
+        flat = [workloads.c12_flame_grf(mech, edge=args.edge, dt=args.dt, cells=idx)]
+        total = n_all
+        wl = f"c12_grf: dodecane random-field flame {args.edge}^3 (T 300-2400 K, Z 0-1), {total} cells"
+    cfg = {"workload": wl + f", synth_c12_53 (53 species + T, {mech.n_reactions} reactions), dt_react "
+                            f"{args.dt:g} s, P 1 atm",
+           "mechanism": C12, "cells": total, "dt_react": args.dt, "rtol": RTOL, "atol": ATOL, "max_order": QMAX,
+           "integrator": "plain GPU BDF, round-based (FP64 state/rates, FP32 Newton inverse + FP64 refinement)",
+           "l2": "inputs larger than L2, state restored from a device copy between steps"}
+    if args.impl == "reference":
+        if rank == 0:
+            rate, n, threads, _ = c12_cpu_rate(mech, flat, args.cpu_seconds)
+            emit({"impl": "reference", "metric": f"cells/s per chem step ({args.workload})", "value": rate,
+                  "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                  "ms_per_step": total / rate * 1e3, "higher_is_better": True, "scaling": "weak",
+                  "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                  "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                   "sample": f"{n} seeded cells of the workload, oracle BDF, extrapolated"},
+                  "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        return
+    import torch
+    import torch.distributed as dist
+    from pelelmex_b200.reactor import Box, ReactorB200
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    props = torch.cuda.get_device_properties(dev)
+    bus = getattr(props, "pci_bus_id", None)
+    bus_id = f"{props.pci_domain_id:08x}:{bus:02x}:{props.pci_device_id:02x}.0" if bus is not None else None
+    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    stream = torch.cuda.current_stream(dev)
+    # device state: working arrays plus pristine copies to restore between steps
+    work, pristine = [], []
+    for f in flat:
+        w = {k: torch.tensor(getattr(f, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
+        w["fct"] = torch.zeros(f.ncells, dtype=torch.float64, device=dev)
+        work.append(w)
+        pristine.append({k: w[k].clone() for k in ("rhoY", "T", "rhoH")})
+    mine_cells = sum(f.ncells for f in flat)
+
+    def restore():
+        for w, p in zip(work, pristine):
+            for k in p:
+                w[k].copy_(p[k])
+
+    if args.workload == "c12_boxes":
+        items = []
+        for (lo, e, f), w in zip(mine, work):
+            v = lambda t, c: t.view(c, e, e, e)  # noqa: E731
+            items.append((Box(lo, (lo[0] + e - 1, e - 1, e - 1)), v(w["rhoY"], N), v(w["frhoY"], N), v(w["T"], 1),
+                          v(w["rhoH"], 1), v(w["frhoH"], 1), v(w["fct"], 1), None))
+
+        def step(stats=False):
+            return r.react_boxes(items, args.dt, stats=stats)
+    else:
+        w0 = work[0]
+
+        def step(stats=False):
+            return r.react_flat(w0["rhoY"], w0["frhoY"], w0["T"], w0["rhoH"], w0["frhoH"], w0["fct"],
+                                dt_react=args.dt, stats=stats)
+    if not args.no_autotune:
+        # seeded sample across all of this rank's cells, flat layout
+        take = []
+        for f in flat:
+            k = max(1, int(round(args.tune_cells * f.ncells / mine_cells)))
+            take.append(f.subset(workloads.sample_cells(f.ncells, min(k, f.ncells), seed=91)))
+        cat = lambda key, ax: torch.tensor(np.concatenate([getattr(t, key) for t in take], axis=ax),  # noqa: E731
+                                           device=dev)
+        t0 = time.perf_counter()
+        tuning, tune_ms = r.autotune(cat("rhoY", 1).contiguous(), cat("frhoY", 1).contiguous(), cat("T", 0),
+                                     cat("rhoH", 0), cat("frhoH", 0), args.dt, max_trials=32)
+        cfg["launch_tuning"] = dict(tuning, sample_ms=round(tune_ms, 3), seconds=round(time.perf_counter() - t0, 2))
+    counters = None
+    for wi in range(args.warmup):
+        restore()
+        res = step(stats=(wi == 0))
+        if wi == 0:
+            counters = res[2]
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = r.kernel_launches()
+    with ClockSampler(bus_id) as clk:
+        for s_ in range(args.steps):
+            restore()
+            ev[s_][0].record(stream)
+            step()
+            ev[s_][1].record(stream)
+        torch.cuda.synchronize()
+    launches = r.kernel_launches() - l0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank != 0:
+        r.close()
+        return
+    cpu = None
+    if not args.no_cpu:
+        rate, n, threads, el = c12_cpu_rate(mech, flat, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} seeded cells of the workload, oracle BDF on {threads} host threads ({el:.1f} s), "
+                         f"extrapolated to cells/s"}
+    emit({"metric": f"cells/s per chem step ({args.workload})", "value": total / (ms * 1e-3), "unit": UNIT,
+          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+          "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; synthetic "
+          "dodecane-shaped mechanism)", "config": cfg, "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches,
+          "clocks": clk.summary(), "step_ms": step_ms,
+          "counters": {k: int(v) for k, v in counters.items()} if counters else None})
+    r.close()
+
+
+def c12_cpu_rate(mech, flat, seconds):
+    """Oracle cells/s on a seeded sample drawn across the workload's fields,
+    grown until the run takes about a third of `seconds`."""
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    o = orc.Oracle(mechmod.flatten(mech))
+    threads = orc.max_threads()
+    total = sum(f.ncells for f in flat)
+    n = max(64, 8 * threads)
+    while True:
+        parts = []
+        for i, f in enumerate(flat):
+            k = max(1, int(round(n * f.ncells / total)))
+            parts.append(f.subset(workloads.sample_cells(f.ncells, min(k, f.ncells), seed=500 + i)))
+        cat = lambda key, ax: np.ascontiguousarray(np.concatenate([getattr(p, key) for p in parts], axis=ax))  # noqa
+        m = sum(p.ncells for p in parts)
+        t0 = time.perf_counter()
+        o.react(cat("rhoY", 1), cat("frhoY", 1), cat("T", 0), cat("rhoH", 0), cat("frhoH", 0), flat[0].dt,
+                rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS, nthreads=threads)
+        el = time.perf_counter() - t0
+        if el >= 0.3 * seconds or m >= total:
+            return m / el, m, threads, el
+        n = min(total, int(n * min(8.0, max(1.5, 0.6 * seconds / max(el, 1e-3)))))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     args.warmup = max(3, args.warmup)
+    if args.dt is None:
+        args.dt = 5e-6 if args.workload == "c12_grf" else 1e-6
+    if args.workload != "flame_ch4":
+        run_dodecane(args, rank, world, local_rank)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -190,3 +190,128 @@ def sample_cells(n_total: int, n_sample: int, seed: int = 12345) -> np.ndarray:
         return np.arange(n_total, dtype=np.int64)
     u = uniform(seed, 0, np.arange(n_total, dtype=np.int64))
     return np.sort(np.argsort(u)[:n_sample]).astype(np.int64)
+
+
+# --------------------------------------------------------------- dodecane
+def _c12_air(mech, Z):
+    """Fuel/air mixing line: n-C12H26 mass fraction Z, the rest air
+    (O2 : N2 = 1 : 3.76 by moles)."""
+    nm = mech.names
+    Xa = np.zeros(mech.n_species)
+    Xa[nm.index("O2")] = 1.0
+    Xa[nm.index("N2")] = 3.76
+    Ya = mechmod.mole_to_mass(mech, (Xa / Xa.sum())[None, :])[0]
+    Y = (1.0 - Z)[:, None] * Ya[None, :]
+    Y[:, nm.index("NC12H26")] += Z
+    return Y
+
+
+def _c12_phi_to_Z(mech, phi):
+    """Fuel mass fraction of n-C12H26/air at equivalence ratio phi
+    (stoichiometric: 18.5 O2 per C12H26)."""
+    mw = mech.mw()
+    nm = mech.names
+    w_f = mw[nm.index("NC12H26")]
+    w_air = 18.5 * (mw[nm.index("O2")] + 3.76 * mw[nm.index("N2")])
+    fa = phi * w_f / w_air
+    return fa / (1.0 + fa)
+
+
+def _c12_products(mech, Z):
+    """Complete-combustion products of the mixture at fuel mass fraction Z:
+    lean -> CO2, H2O, excess O2, N2; rich -> the oxygen deficit goes to CO
+    then H2, any fuel beyond that stays unburnt."""
+    nm = mech.names
+    mw = mech.mw()
+    Y0 = _c12_air(mech, Z)
+    n_f = Y0[:, nm.index("NC12H26")] / mw[nm.index("NC12H26")]
+    n_o2 = Y0[:, nm.index("O2")] / mw[nm.index("O2")]
+    n_n2 = Y0[:, nm.index("N2")] / mw[nm.index("N2")]
+    burn = np.minimum(n_f, n_o2 / 12.5)          # fuel that at least reaches CO + H2O
+    o2 = n_o2 - 12.5 * burn
+    co = 12.0 * burn
+    h2o = 13.0 * burn
+    to_co2 = np.minimum(co, 2.0 * o2)            # remaining O2 oxidises CO
+    co -= to_co2
+    o2 -= 0.5 * to_co2
+    X = np.zeros((Z.size, mech.n_species))
+    X[:, nm.index("NC12H26")] = n_f - burn
+    X[:, nm.index("CO2")] = to_co2
+    X[:, nm.index("CO")] = co
+    X[:, nm.index("H2O")] = h2o
+    X[:, nm.index("O2")] = o2
+    X[:, nm.index("N2")] = n_n2
+    return mechmod.mole_to_mass(mech, X / X.sum(axis=1, keepdims=True))
+
+
+def c12_boxes(mech, seed: int = 3, dt: float = 1e-6, nbox: int = 40, edges=(16, 32, 64), box_cells=None):
+    """AMR-like dodecane box list: `nbox` cubic boxes with edges drawn from
+    `edges`; the first half cold and inert (T ~ U[300, 600] K), the second
+    half igniting (T ~ U[900, 1400] K); per cell phi ~ U[0.5, 2]
+    (n-C12H26/air), +-2% noise on Y.  Returns [(lo, edge, Field)]; lo places
+    the boxes side by side along x.  box_cells (optional) caps the cells
+    generated per box (a seeded subset, for parity samples)."""
+    out = []
+    bidx = np.arange(nbox, dtype=np.int64)
+    pick = np.minimum((uniform(seed, 0, bidx) * len(edges)).astype(np.int64), len(edges) - 1)
+    x0 = 0
+    for b in range(nbox):
+        e = int(edges[pick[b]])
+        shape = (e, e, e)
+        c = _cells(shape, None)
+        if box_cells is not None and box_cells < c.size:
+            c = sample_cells(c.size, box_cells, seed=seed * 1000 + b)
+        key = seed * 4096 + b
+        cold = b < nbox // 2
+        u = uniform(key, 0, c)
+        T = (300.0 + 300.0 * u) if cold else (900.0 + 500.0 * u)
+        phi = 0.5 + 1.5 * uniform(key, 1, c)
+        Y = _c12_air(mech, _c12_phi_to_Z(mech, phi))
+        for k in range(mech.n_species):
+            Y[:, k] *= 1.0 + 0.04 * (uniform(key, 10 + k, c) - 0.5)
+        Y /= Y.sum(axis=1, keepdims=True)
+        out.append(((x0, 0, 0), e, _finish(mech, Y, T, dt, shape if box_cells is None else (c.size,),
+                                           f"c12_box{b}_{'cold' if cold else 'ignite'}")))
+        x0 += e
+    return out
+
+
+def _grf(seed: int, draw: int, cells: np.ndarray, edge: int, modes: int = 64, ell: float = 16.0):
+    """Smoothed Gaussian random field on an edge^3 grid, evaluated cell by
+    cell: a sum of `modes` random Fourier modes with wave vectors drawn from
+    the spectrum of a Gaussian filter of width ell cells (so the field is a
+    Gaussian-filtered white noise up to the mode sampling), normalised to
+    zero mean and unit variance."""
+    m = np.arange(modes, dtype=np.int64)
+    g = []
+    for d in range(3):
+        u1 = np.maximum(uniform(seed, 1000 * draw + 2 * d, m), 1e-300)
+        u2 = uniform(seed, 1000 * draw + 2 * d + 1, m)
+        g.append(np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2) / ell)   # Box-Muller
+    kx, ky, kz = g
+    ph = 2.0 * np.pi * uniform(seed, 1000 * draw + 7, m)
+    i = (cells % edge).astype(np.float64)
+    j = ((cells // edge) % edge).astype(np.float64)
+    k = (cells // (edge * edge)).astype(np.float64)
+    f = np.zeros(cells.size)
+    for q in range(modes):
+        f += np.cos(kx[q] * i + ky[q] * j + kz[q] * k + ph[q])
+    return f * np.sqrt(2.0 / modes)
+
+
+def c12_flame_grf(mech, edge: int = 256, seed: int = 6, dt: float = 5e-6, cells=None) -> Field:
+    """Turbulent-flame-like dodecane field: T in [300, 2400] K and mixture
+    fraction Z in [0, 1] (air to n-C12H26) from two seeded smoothed Gaussian
+    random fields mapped through the normal CDF; the composition blends the
+    mixing line and the complete-combustion products at the local Z with
+    progress (T - 300) / 2100."""
+    from scipy.special import ndtr as cdf
+    shape = (edge, edge, edge)
+    c = _cells(shape, cells)
+    T = 300.0 + 2100.0 * cdf(_grf(seed, 0, c, edge))
+    Z = cdf(_grf(seed, 1, c, edge))
+    prog = (T - 300.0) / 2100.0
+    Y = (1.0 - prog)[:, None] * _c12_air(mech, Z) + prog[:, None] * _c12_products(mech, Z)
+    Y = np.maximum(Y, 0.0)
+    Y /= Y.sum(axis=1, keepdims=True)
+    return _finish(mech, Y, T, dt, shape, "c12_flame_grf")

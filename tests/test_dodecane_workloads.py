@@ -1,0 +1,101 @@
+"""The dodecane workloads: the AMR-like box list (40 boxes of edges 16 / 32
+/ 64, half cold and inert, half igniting) and the turbulent-flame-like
+random field (T and mixture fraction from smoothed Gaussian random
+fields).  CPU tests check the generators; GPU tests react reduced versions
+through the box API (all boxes in one launch) and the flat API and compare
+with the CPU oracle at the reactor's parity tolerances."""
+import numpy as np
+import pytest
+
+from pelelmex_b200 import mechanism as M, workloads as W
+
+MECH = "synth_c12_53"
+
+
+def test_box_list_generator():
+    mech = M.builtin(MECH)
+    bl = W.c12_boxes(mech, nbox=8, edges=(4, 8))
+    assert len(bl) == 8
+    x = 0
+    for b, (lo, e, f) in enumerate(bl):
+        assert lo == (x, 0, 0) and e in (4, 8) and f.ncells == e ** 3
+        x += e
+        Y = f.rhoY / f.rhoY.sum(axis=0)
+        assert np.allclose(Y.sum(axis=0), 1.0)
+        if b < 4:
+            assert f.T.min() >= 300.0 and f.T.max() <= 600.0
+        else:
+            assert f.T.min() >= 900.0 and f.T.max() <= 1400.0
+        # fuel/air at phi in [0.5, 2] with +-2% noise
+        z = Y[mech.names.index("NC12H26")]
+        assert z.min() > 0.95 * W._c12_phi_to_Z(mech, np.array([0.5]))[0]
+        assert z.max() < 1.05 * W._c12_phi_to_Z(mech, np.array([2.0]))[0]
+    # a seeded subset regenerates the same cells
+    sub = W.c12_boxes(mech, nbox=8, edges=(4, 8), box_cells=16)
+    for b, ((lo, e, f), (_, _, g)) in enumerate(zip(bl, sub)):
+        idx = W.sample_cells(e ** 3, 16, seed=3 * 1000 + b)
+        assert np.array_equal(g.T, f.T[idx]) and np.array_equal(g.rhoY, f.rhoY[:, idx])
+
+
+def test_random_field_generator():
+    mech = M.builtin(MECH)
+    edge = 32
+    f = W.c12_flame_grf(mech, edge=edge, dt=5e-6)
+    assert f.T.min() >= 300.0 and f.T.max() <= 2400.0
+    assert f.T.std() > 200.0
+    Y = f.rhoY / f.rhoY.sum(axis=0)
+    assert np.allclose(Y.sum(axis=0), 1.0) and (Y >= 0).all()
+    # smooth: neighbouring cells along x are strongly correlated
+    T3 = f.T.reshape(edge, edge, edge)
+    r = np.corrcoef(T3[:, :, :-1].ravel(), T3[:, :, 1:].ravel())[0, 1]
+    assert r > 0.9
+    idx = np.array([0, 5, 777, edge ** 3 - 1])
+    g = W.c12_flame_grf(mech, edge=edge, dt=5e-6, cells=idx)
+    assert np.array_equal(g.T, f.T[idx]) and np.array_equal(g.rhoY, f.rhoY[:, idx])
+
+
+@pytest.mark.gpu
+def test_box_list_one_launch_matches_oracle(orc_cache):
+    torch = pytest.importorskip("torch")
+    from pelelmex_b200.reactor import Box, ReactorB200
+    from test_gpu_parity import T_RTOL, Y_ATOL, _dev
+    mech = M.builtin(MECH)
+    N = mech.n_species
+    bl = W.c12_boxes(mech, nbox=6, edges=(4, 8))
+    r = ReactorB200(MECH, rtol=1e-8, atol=1e-12, max_order=5).init()
+    items, fabs = [], []
+    for lo, e, f in bl:
+        box = Box(lo, (lo[0] + e - 1, e - 1, e - 1))
+        fb = [_dev(f.rhoY.reshape(N, e, e, e)), _dev(f.frhoY.reshape(N, e, e, e)), _dev(f.T.reshape(1, e, e, e)),
+              _dev(f.rhoH.reshape(1, e, e, e)), _dev(f.frhoH.reshape(1, e, e, e)),
+              torch.zeros((1, e, e, e), dtype=torch.float64, device="cuda:0")]
+        mk = torch.ones((1, e, e, e), dtype=torch.int32, device="cuda:0")
+        items.append((box, *fb, mk))
+        fabs.append(fb)
+    n0 = r.kernel_launches()
+    r.react_boxes(items, 1e-6)
+    torch.cuda.synchronize()
+    assert r.kernel_launches() > n0
+    orc = orc_cache(MECH)
+    for (lo, e, f), fb in zip(bl, fabs):
+        o = orc.react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12, max_order=5)
+        assert o["nfail"] == 0
+        T = fb[2].reshape(-1).cpu().numpy()
+        rY = fb[0].reshape(N, -1).cpu().numpy()
+        assert (np.abs(T - o["T"]) / o["T"]).max() <= T_RTOL, f.name
+        assert (np.abs(rY - o["rhoY"]).max(axis=0) / f.rhoY.sum(axis=0)).max() <= Y_ATOL, f.name
+        assert (fb[5].reshape(-1).cpu().numpy() > 0).all()
+    r.close()
+
+
+@pytest.mark.gpu
+def test_random_field_sample_matches_oracle(orc_cache):
+    pytest.importorskip("torch")
+    from test_gpu_parity import T_RTOL, Y_ATOL, run_gpu
+    mech = M.builtin(MECH)
+    f = W.c12_flame_grf(mech, cells=W.sample_cells(256 ** 3, 256, seed=61), dt=5e-6)
+    g = run_gpu(MECH, f)
+    o = orc_cache(MECH).react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-8, atol=1e-12, max_order=5)
+    assert (g["status"] == 0).all() and o["nfail"] == 0
+    assert (np.abs(g["T"] - o["T"]) / o["T"]).max() <= T_RTOL
+    assert (np.abs(g["rhoY"] - o["rhoY"]).max(axis=0) / f.rhoY.sum(axis=0)).max() <= Y_ATOL
