@@ -66,6 +66,13 @@ def parse():
     return p.parse_args()
 
 
+# DRAM bytes (read + write) of rk_ctrl per cell it processes: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum summed over every rk_ctrl
+# launch of the kernel-profile pass of `bench.py --cells 262144`, divided by
+# the cells those launches processed.
+CTRL_DRAM_BYTES_PER_CELL = 10055.0
+
+
 def workload_config(args):
     sub = f" ({args.cells} seeded random cells)" if args.cells else ""
     return {"workload": f"flame_ch4 {args.edge}^3{sub} drm19-shaped (synth_ch4_21: 21 species + T, 84 reactions), "
@@ -420,27 +427,59 @@ def run_b200(args, rank, world, local_rank):
         e2e = {"value": world * nc / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
 
-    # roofline of the react kernel (FP64 algorithmic flops per launch)
+    # per-kernel profile: one more react of the same field with CUDA events
+    # around every launch (kernel by kernel, outside the timed region)
+    restore()
+    torch.cuda.nvtx.range_push("kernel_profile_pass")
+    r.profile_begin()
+    r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
+    prof = r.profile_end()
+    torch.cuda.nvtx.range_pop()
+    kernels, tot_ms = {}, sum(v["ms"] for k, v in prof.items() if k != "complete")
+    for k in ("start", "rhs", "ctrl", "jac", "gj", "ctrl_setup"):
+        v = prof[k]
+        b = perfmodel.kernel_bytes(k, N) * v["cells"]
+        if k == "jac":
+            b += perfmodel.jac_refresh_bytes(N) * counters["nje"]
+        kernels[k] = dict(v, share=v["ms"] / tot_ms if tot_ms else None,
+                          algorithmic_gbs=(b / (v["ms"] * 1e-3) / 1e9) if v["ms"] else None, bytes=b)
+    # dominant kernel: rk_ctrl (both of its launches per round)
+    c_ms = kernels["ctrl"]["ms"] + kernels["ctrl_setup"]["ms"]
+    c_launch = kernels["ctrl"]["launches"] + kernels["ctrl_setup"]["launches"]
+    c_cells = kernels["ctrl"]["cells"] + kernels["ctrl_setup"]["cells"]
+    c_bytes = kernels["ctrl"]["bytes"] + kernels["ctrl_setup"]["bytes"]
+    hbm_peak, hbm_src = None, None
+    mp = ROOT / "MEASURED_PEAKS.json"
+    if mp.exists():
+        try:
+            hbm_peak = json.loads(mp.read_text()).get("hbm_gbs")
+            hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except (ValueError, OSError):
+            hbm_peak = None
+    if hbm_peak is None:
+        hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    c_gbs = c_bytes / (c_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": c_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": c_gbs / hbm_peak,
+            "traffic": (CTRL_DRAM_BYTES_PER_CELL * c_cells / c_launch) if CTRL_DRAM_BYTES_PER_CELL else None,
+            "kernel": "rk_ctrl (step control + FP32-inverse Newton solve with FP64 refinement), both launches "
+                      "of each round",
+            "peak_source": hbm_src, "launches": c_launch, "avg_launch_ms": c_ms / c_launch,
+            "algorithmic_bytes_per_cell": perfmodel.kernel_bytes("ctrl", N), "cells_per_launch": c_cells / c_launch,
+            "share_of_react_kernels": c_ms / tot_ms, "profile_complete": prof["complete"],
+            "kernels": kernels}
+
+    # FP64 view of the whole react call (algorithmic flops per call)
     counts = perfmodel.op_counts(r.flat)
     cn = {k: counters[k] / nc for k in ("nfe", "nje", "nlu", "nst")}
     fl_cell = perfmodel.flops_per_cell(counts, cn["nfe"], cn["nje"], cn["nlu"], cn["nfe"], cn["nst"])
     achieved = fl_cell * nc / (ms * 1e-3) / 1e12
     peak = fp64_peak_tflops(torch, dev)
-    traffic = None
-    tj = ROOT / "profiles" / "traffic.json"
-    if tj.exists():
-        try:
-            tr = json.loads(tj.read_text())
-            if tr.get("edge") == args.edge and tr.get("dt") == args.dt:
-                traffic = tr.get("bytes_per_launch")
-        except (ValueError, OSError):
-            traffic = None
-    roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "one react call: rk_rhs / rk_ctrl / rk_jac / rk_gj rounds",
-            "peak_source": "measured live: cuBLAS DGEMM 8192^3 best of 5 (FP64 has no entry in the measured-peaks "
-                           "file)",
-            "flops_per_cell": fl_cell, "per_cell_counters": cn,
-            "hbm_algorithmic_bytes_per_launch": perfmodel.bytes_per_cell(N) * nc}
+    roof["fp64_view"] = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "kernel": "one react call: rk_rhs / rk_ctrl / rk_jac / rk_gj rounds",
+                         "peak_source": "measured live: cuBLAS DGEMM 8192^3 best of 5 (FP64 has no entry in the "
+                                        "measured-peaks file)",
+                         "flops_per_cell": fl_cell, "per_cell_counters": cn,
+                         "io_bytes_per_call": perfmodel.bytes_per_cell(N) * nc}
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu:
@@ -546,9 +585,11 @@ def run_dodecane(args, rank, world, local_rank):
                                 dt_react=args.dt, stats=stats)
     if not args.no_autotune:
         # seeded sample across all of this rank's cells, flat layout
+        # igniting random-field cells cost ~20x a box-list cell: a smaller sample
+        tune_cells = min(args.tune_cells, 16384 if args.workload == "c12_grf" else 65536)
         take = []
         for f in flat:
-            k = max(1, int(round(args.tune_cells * f.ncells / mine_cells)))
+            k = max(1, int(round(tune_cells * f.ncells / mine_cells)))
             take.append(f.subset(workloads.sample_cells(f.ncells, min(k, f.ncells), seed=91)))
         cat = lambda key, ax: torch.tensor(np.concatenate([getattr(t, key) for t in take], axis=ax),  # noqa: E731
                                            device=dev)

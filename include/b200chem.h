@@ -239,6 +239,31 @@ int b200chem_autotune(b200chem_handle h, const double* rhoY, const double* extF_
                       const double* rhoH, const double* extF_rhoH, int64_t ncells, double dt_react,
                       int32_t max_trials, void* stream, b200chem_tuning* best, double* best_ms);
 
+/* ---------------------------------------------------- kernel profile
+ * Per-kernel CUDA-event timing of the round-based integrator (no reference
+ * counterpart).  Between profile_begin and profile_end every react call
+ * launches its kernels one by one (no graph replay), each bracketed by two
+ * events, and records how many cells each launch processed. */
+enum {
+  B200CHEM_PROF_START = 0,       /* rk_start: load, validate, initialise   */
+  B200CHEM_PROF_RHS = 1,         /* rk_rhs: right-hand sides               */
+  B200CHEM_PROF_CTRL = 2,        /* rk_ctrl after the right-hand sides     */
+  B200CHEM_PROF_JAC = 3,         /* rk_jac: analytic Jacobians             */
+  B200CHEM_PROF_GJ = 4,          /* rk_gj: Newton-matrix inverses          */
+  B200CHEM_PROF_CTRL_SETUP = 5,  /* rk_ctrl after a setup                  */
+  B200CHEM_PROF_KINDS = 8
+};
+typedef struct b200chem_kernel_profile {
+  int64_t launches[B200CHEM_PROF_KINDS];
+  int64_t cells[B200CHEM_PROF_KINDS];  /* list entries processed, summed over launches */
+  double ms[B200CHEM_PROF_KINDS];      /* summed event time of the launches           */
+  int32_t complete;                    /* 0: more launches than the record holds      */
+  int32_t reserved;
+} b200chem_kernel_profile;
+
+int b200chem_profile_begin(b200chem_handle h);
+int b200chem_profile_end(b200chem_handle h, b200chem_kernel_profile* out);
+
 const char* b200chem_last_error(void);
 int b200chem_version(void);
 

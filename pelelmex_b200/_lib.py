@@ -57,6 +57,14 @@ class Tuning(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+PROF_KINDS = ("start", "rhs", "ctrl", "jac", "gj", "ctrl_setup")
+
+
+class KernelProfile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64 * 8), ("cells", ctypes.c_int64 * 8), ("ms", ctypes.c_double * 8),
+                ("complete", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class B200ChemError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"b200chem error {code}: {msg}")
@@ -110,7 +118,10 @@ def load(path: os.PathLike | None = None):
     L.b200chem_autotune.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int64,
                                     ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Tuning),
                                     ctypes.POINTER(ctypes.c_double)]
-    for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune"):
+    L.b200chem_profile_begin.argtypes = [ctypes.c_void_p]
+    L.b200chem_profile_end.argtypes = [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]
+    for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune", "b200chem_profile_begin",
+                 "b200chem_profile_end"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):
         f = getattr(L, name)

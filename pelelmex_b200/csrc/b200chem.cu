@@ -217,6 +217,20 @@ struct b200chem_reactor {
   cudaStream_t cap_stream = nullptr;  // private stream the round graph is captured on
   cudaGraphExec_t rgraph = nullptr;   // executable graph of rounds_per_check rounds
   int rgraph_rounds = 0;              // rounds in rgraph
+  // per-kernel profile of the round integrator (b200chem_profile_begin/end)
+  struct ProfRec {
+    int kind;
+    int slot;  // index into h_pcnt (-1: cell count known on the host)
+    long long cells;
+    cudaEvent_t e0, e1;
+  };
+  bool prof_on = false;
+  bool prof_overflow = false;
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  int* h_pcnt = nullptr;  // pinned list counts copied before each profiled launch
+  int pcnt_used = 0;
 };
 
 namespace b200 {
@@ -362,6 +376,43 @@ int tuned_grid(int max_grid, int sm_count, int per_sm) {
 // step control (Newton update, error test, next prediction) appending to
 // list_out and to the setup list, Jacobian and iteration-matrix inversion of
 // the setup list, step control of the cells back from their setup.
+constexpr int kProfCountSlots = 1 << 16;
+
+cudaEvent_t prof_event(b200chem_reactor* h) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    h->ev_pool.push_back(e);
+  }
+  return h->ev_pool[h->ev_used++];
+}
+
+// One kernel of the round integrator; when the handle profiles, the launch is
+// bracketed by two events and the count of the list it processes is copied
+// to the host first (stream-ordered, so it is the count the kernel sees).
+int launch_kernel(b200chem_reactor* h, int lut, int what, int prof_kind, const RoundsParams& R, const RoundsGrids& G,
+                  int after_rhs, const int* cnt, long long host_cells, cudaStream_t st) {
+  if (!h->prof_on || h->prof_overflow) {
+    CK(rounds_launch(h->N, lut, what, R, G, after_rhs, st));
+    return 0;
+  }
+  b200chem_reactor::ProfRec rec{prof_kind, -1, host_cells, prof_event(h), prof_event(h)};
+  if (!rec.e0 || !rec.e1 || (cnt && h->pcnt_used >= kProfCountSlots)) {
+    h->prof_overflow = true;
+    CK(rounds_launch(h->N, lut, what, R, G, after_rhs, st));
+    return 0;
+  }
+  if (cnt) {
+    rec.slot = h->pcnt_used++;
+    CK(cudaMemcpyAsync(h->h_pcnt + rec.slot, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaEventRecord(rec.e0, st));
+  CK(rounds_launch(h->N, lut, what, R, G, after_rhs, st));
+  CK(cudaEventRecord(rec.e1, st));
+  h->prof.push_back(rec);
+  return 0;
+}
+
 int enqueue_round(b200chem_reactor* h, int lut, RoundsParams R, const RoundsGrids& G, int* list_in, int* cnt_in,
                   int* list_out, int* cnt_out, int* list_setup, int* cnt_setup, cudaStream_t st) {
   R.list_in = list_in;
@@ -370,17 +421,17 @@ int enqueue_round(b200chem_reactor* h, int lut, RoundsParams R, const RoundsGrid
   R.cnt_out = cnt_out;
   R.list_setup = list_setup;
   R.cnt_setup = cnt_setup;
-  CK(rounds_launch(h->N, lut, kRoundsRhs, R, G, 0, st));
+  int err = launch_kernel(h, lut, kRoundsRhs, B200CHEM_PROF_RHS, R, G, 0, cnt_in, 0, st);
+  if (err) return err;
   CK(cudaMemsetAsync(cnt_out, 0, sizeof(int), st));
   CK(cudaMemsetAsync(cnt_setup, 0, sizeof(int), st));
-  CK(rounds_launch(h->N, lut, kRoundsCtrl, R, G, 1, st));
+  if ((err = launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL, R, G, 1, cnt_in, 0, st))) return err;
   R.list_in = list_setup;
   R.cnt_in = cnt_setup;
-  CK(rounds_launch(h->N, lut, kRoundsJac, R, G, 0, st));
-  CK(rounds_launch(h->N, lut, kRoundsGj, R, G, 0, st));
+  if ((err = launch_kernel(h, lut, kRoundsJac, B200CHEM_PROF_JAC, R, G, 0, cnt_setup, 0, st))) return err;
+  if ((err = launch_kernel(h, lut, kRoundsGj, B200CHEM_PROF_GJ, R, G, 0, cnt_setup, 0, st))) return err;
   // cells coming back from a setup always ask for a right-hand side next
-  CK(rounds_launch(h->N, lut, kRoundsCtrl, R, G, 0, st));
-  return 0;
+  return launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL_SETUP, R, G, 0, cnt_setup, 0, st);
 }
 
 // Captures `rounds` rounds (an even number: the two slot lists swap roles
@@ -446,7 +497,8 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   G.jac = tuned_grid(h->rgrid.jac, h->sm_count, T.jac_ctas_per_sm);
   G.gj = tuned_grid(h->rgrid.gj, h->sm_count, T.gj_ctas_per_sm);
   const int per_check = T.rounds_per_check > 0 ? T.rounds_per_check : kRoundsCheckEvery;
-  const bool graph = T.use_graph != 2;
+  // a profiled call launches kernel by kernel (events between the launches)
+  const bool graph = T.use_graph != 2 && !h->prof_on;
   // chunk capacity from the state budget (and the free device memory)
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
@@ -494,7 +546,8 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     R.cnt_out = cnt[0];
     R.list_setup = listS;
     R.cnt_setup = cntS;
-    CK(rounds_launch(h->N, lut, kRoundsStart, R, G, 0, st));
+    err = launch_kernel(h, lut, kRoundsStart, B200CHEM_PROF_START, R, G, 0, nullptr, R.nchunk, st);
+    if (err) return err;
     h->launches++;
     if (graph) {
       err = capture_rounds(h, lut, R, G, per_check, lst, cnt, listS, cntS);
@@ -1093,6 +1146,35 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
 
 int64_t b200chem_kernel_launches(b200chem_handle h) { return h ? h->launches : -1; }
 
+int b200chem_profile_begin(b200chem_handle h) {
+  if (!h) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!h->h_pcnt) CK(cudaMallocHost(&h->h_pcnt, sizeof(int) * kProfCountSlots));
+  h->prof.clear();
+  h->ev_used = 0;
+  h->pcnt_used = 0;
+  h->prof_overflow = false;
+  h->prof_on = true;
+  return 0;
+}
+
+int b200chem_profile_end(b200chem_handle h, b200chem_kernel_profile* out) {
+  if (!h || !out) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!h->prof_on) return set_err(B200CHEM_EINVAL, "profile_end without profile_begin");
+  h->prof_on = false;
+  memset(out, 0, sizeof(*out));
+  for (const auto& r : h->prof) {
+    CK(cudaEventSynchronize(r.e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+    out->launches[r.kind] += 1;
+    out->ms[r.kind] += ms;
+    out->cells[r.kind] += (r.slot >= 0) ? h->h_pcnt[r.slot] : r.cells;
+  }
+  out->complete = h->prof_overflow ? 0 : 1;
+  h->prof.clear();
+  return 0;
+}
+
 int b200chem_get_tuning(b200chem_handle h, b200chem_tuning* t) {
   if (!h || !t) return set_err(B200CHEM_EINVAL, "bad arguments");
   *t = h->tune;
@@ -1261,6 +1343,8 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
   if (h->h_cmech) cudaFreeHost(h->h_cmech);
   if (h->rgraph) cudaGraphExecDestroy(h->rgraph);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->h_pcnt) cudaFreeHost(h->h_pcnt);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   delete h;
   return 0;

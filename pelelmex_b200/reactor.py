@@ -209,6 +209,23 @@ class ReactorB200:
             float(dt_react), int(max_trials), _stream_ptr(stream), ctypes.byref(best), ctypes.byref(ms)))
         return {f: int(getattr(best, f)) for f in self.TUNING_FIELDS}, float(ms.value)
 
+    def profile_begin(self):
+        """Per-kernel event timing of the following react calls (round-based
+        integrator; kernels are then launched one by one, not from a graph)."""
+        self._need()
+        _lib.check(_lib.load().b200chem_profile_begin(self._h))
+
+    def profile_end(self) -> dict:
+        """{kind: {"launches", "cells", "ms"}} since profile_begin, kinds
+        start / rhs / ctrl / jac / gj / ctrl_setup; plus "complete"."""
+        self._need()
+        p = _lib.KernelProfile()
+        _lib.check(_lib.load().b200chem_profile_end(self._h, ctypes.byref(p)))
+        out = {k: {"launches": int(p.launches[i]), "cells": int(p.cells[i]), "ms": float(p.ms[i])}
+               for i, k in enumerate(_lib.PROF_KINDS)}
+        out["complete"] = bool(p.complete)
+        return out
+
     def close(self):
         if self._h:
             _lib.load().b200chem_destroy(self._h)

@@ -106,3 +106,30 @@ def test_autotune_valid_and_same_results():
     assert tuning["rounds_per_check"] in (0, 2, 4, 8, 16) and tuning["use_graph"] in (0, 1, 2)
     assert got["tuning"] == tuning
     _same(f, got, ref)
+
+
+@pytest.mark.gpu
+def test_kernel_profile_counts_match_integrator_counters():
+    from pelelmex_b200.reactor import ReactorB200
+    f = _field(4096, 13)
+    dev = torch.device("cuda:0")
+    r = ReactorB200("synth_ch4_21", rtol=1e-8, atol=1e-12, kernel="rounds").init(2, f.ncells)
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
+    rhoY, T, rhoH, fY, fH = d(f.rhoY), d(f.T), d(f.rhoH), d(f.frhoY), d(f.frhoH)
+    r.profile_begin()
+    _, _, st = r.react_flat(rhoY, fY, T, rhoH, fH, dt_react=f.dt, stats=True)
+    p = r.profile_end()
+    assert p["complete"]
+    assert p["start"]["launches"] == 1 and p["start"]["cells"] == f.ncells
+    rounds = p["rhs"]["launches"]
+    assert rounds >= st["max_nfe"] and all(p[k]["launches"] == rounds for k in ("ctrl", "jac", "gj", "ctrl_setup"))
+    # every right-hand side is consumed by one control pass; every setup by one Jacobian, inverse and control pass
+    assert p["rhs"]["cells"] == p["ctrl"]["cells"] == st["nfe"]
+    assert p["jac"]["cells"] == p["gj"]["cells"] == p["ctrl_setup"]["cells"] == st["nlu"]
+    assert all(p[k]["ms"] > 0 for k in ("start", "rhs", "ctrl", "gj"))
+    # profiling changes the launch mode only, not the result
+    rY2, T2, rH2 = d(f.rhoY), d(f.T), d(f.rhoH)
+    r.react_flat(rY2, fY, T2, rH2, fH, dt_react=f.dt)
+    torch.cuda.synchronize()
+    assert torch.equal(T, T2) and torch.equal(rhoY, rY2)
+    r.close()
