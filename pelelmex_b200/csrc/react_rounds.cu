@@ -384,8 +384,14 @@ __global__ void __launch_bounds__(128) rk_start(RoundsParams R) {
   }
 }
 
+// Minimum resident CTAs (of 64 threads) per SM requested for the
+// right-hand-side kernel: bounds its registers per thread.
+#ifndef B200_RHS_MIN_CTAS
+#define B200_RHS_MIN_CTAS 6
+#endif
+
 template <int NS>
-__global__ void __launch_bounds__(kRoundsRhsBlock) rk_rhs(RoundsParams R) {
+__global__ void __launch_bounds__(kRoundsRhsBlock, B200_RHS_MIN_CTAS) rk_rhs(RoundsParams R) {
   constexpr int n = NS + 1;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ DevMech s_mech;
@@ -843,8 +849,9 @@ cudaError_t rounds_grids(const RoundsSetupLayout& SL, int sm_count, RoundsGrids*
   cudaError_t e = rounds_setup_attrs<NS, LUT>(SL);
   if (e != cudaSuccess) return e;
   int b = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_rhs<NS>, kRoundsRhsBlock,
-                                                         rhs_smem<NS>(kRoundsRhsBlock))) != cudaSuccess)
+  // grid sized for the generated right-hand side (no shared memory); the
+  // table forms run the same grid-stride loop with fewer CTAs resident
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_rhs<NS>, kRoundsRhsBlock, 0)) != cudaSuccess)
     return e;
   G->rhs = std::max(1, b) * sm_count;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, rk_ctrl<NS, LUT>, 128, 0)) != cudaSuccess) return e;
@@ -870,7 +877,8 @@ cudaError_t rounds_launch_t(int what, const RoundsParams& R, const RoundsGrids& 
       rk_start<NS><<<G.start, 128, 0, st>>>(R);
       break;
     case kRoundsRhs:
-      rk_rhs<NS><<<G.rhs, kRoundsRhsBlock, rhs_smem<NS>(kRoundsRhsBlock), st>>>(R);
+      // the generated right-hand side keeps everything in registers
+      rk_rhs<NS><<<G.rhs, kRoundsRhsBlock, R.gen_mech ? 0 : rhs_smem<NS>(kRoundsRhsBlock), st>>>(R);
       break;
     case kRoundsCtrl:
       rk_ctrl<NS, LUT><<<G.ctrl, 128, 0, st>>>(R, after_rhs);

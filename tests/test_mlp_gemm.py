@@ -40,7 +40,9 @@ def gemm(A, B, bias=None, epi=EPI_F32, aux=None, n_valid=0):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 16, 16), (128, 32, 32), (256, 256, 256), (384, 32, 256), (256, 256, 1024),
-                                   (128, 512, 64), (1024, 256, 32)])
+                                   (128, 512, 64), (1024, 256, 32),
+                                   # many tiles per CTA: the two accumulators and the stage ring wrap around
+                                   (128 * 301, 256, 256), (128 * 450, 32, 256), (128 * 333, 256, 16)])
 def test_gemm_f32_matches_torch(M, N, K):
     g = torch.Generator(device=DEV).manual_seed(M * 7 + N * 3 + K)
     A = torch.randn((M, K), device=DEV, generator=g).to(torch.bfloat16)
