@@ -532,39 +532,57 @@ __device__ __forceinline__ int reg_gj_inverse(const double* J, int ldj, const do
     const double mij = ((lane == j) ? 1.0 : 0.0) - gamma * (row ? J[j * ldj + lane] : 0.0);
     a[j] = row ? (LUT)(kScaled ? mij * di * rdj : mij) : (LUT)0;
   }
+  // Pivot search by one warp reduction: key = the bits of |a[k]| (FP32; the
+  // high word for FP64) with the low 5 bits replaced by (31 - lane), so the
+  // maximum picks the largest magnitude (to 2^-18 relative in FP32, 2^-15 in
+  // FP64) and, among equals, the lowest lane.
+  // The pivot row goes through shared memory (two buffers, alternating per
+  // step, 16-byte chunks) and every row, the pivot row included, is updated
+  // by one FMA per column: a_ij -= g_i * a_pj with g_i = a_ik / a_pk off the
+  // pivot row and g_p = 1 - 1 / a_pk on it (which scales the pivot row by
+  // 1 / a_pk); column k is set last (1 / a_pk on the pivot row, -g_i off it).
+  constexpr int kVec = 16 / (int)sizeof(LUT);      // LUTs per 16-byte chunk
+  constexpr int kChunks = (n + kVec - 1) / kVec;
+  constexpr int kBuf = 32;                         // LUTs per row buffer (>= kChunks * kVec)
+  static_assert(kChunks * kVec <= kBuf, "row buffer");
   unsigned used = 0;
   int mystep = -1;
 #pragma unroll
   for (int k = 0; k < n; ++k) {
-    LUT best = (row && !((used >> lane) & 1u)) ? fabs(a[k]) : (LUT)-1;
-    int bi = lane;
+    LUT* buf = Xs + (k & 1) * kBuf;
+    unsigned key = 0u;
+    if (row && !((used >> lane) & 1u)) {
+      unsigned bits;
+      if constexpr (sizeof(LUT) == 4) bits = __float_as_uint(fabsf((float)a[k]));
+      else bits = (unsigned)__double2hiint(fabs((double)a[k]));
+      key = (bits & ~31u) | (unsigned)(31 - lane);
+    }
+    const unsigned kmax = __reduce_max_sync(kFull, key);
+    if ((kmax >> 5) == 0u) return k + 1;  // no nonzero candidate: singular (warp-uniform)
+    const int p = 31 - (int)(kmax & 31u);
+    used |= 1u << p;
+    if (lane == p) {
+      mystep = k;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const LUT ov = __shfl_xor_sync(kFull, best, o);
-      const int oi = __shfl_xor_sync(kFull, bi, o);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
+      for (int c = 0; c < kChunks; ++c) {
+        LUT t[kVec];
+#pragma unroll
+        for (int e = 0; e < kVec; ++e) t[e] = (c * kVec + e < n) ? a[c * kVec + e] : (LUT)0;
+        *reinterpret_cast<uint4*>(buf + c * kVec) = *reinterpret_cast<const uint4*>(t);
       }
     }
-    if (!(best > (LUT)0)) return k + 1;  // zero or NaN pivot: singular (warp-uniform)
-    const int p = bi;
-    used |= 1u << p;
-    if (lane == p) mystep = k;
-    const LUT inv = (LUT)1 / __shfl_sync(kFull, a[k], p);
-    const LUT f = a[k];
-    if (lane == p) {
-      a[k] = (LUT)1;
+    __syncwarp();
+    LUT pr[kChunks * kVec];
 #pragma unroll
-      for (int j = 0; j < n; ++j) a[j] *= inv;
-    } else {
-      a[k] = (LUT)0;
-    }
+    for (int c = 0; c < kChunks; ++c) *reinterpret_cast<uint4*>(pr + c * kVec) = *reinterpret_cast<const uint4*>(buf + c * kVec);
+    const LUT pv = pr[k];
+    if (!(fabs(pv) > (LUT)0) || isnan(pv)) return k + 1;  // zero or NaN pivot (warp-uniform)
+    const LUT inv = (LUT)1 / pv;
+    const LUT gi = (lane == p) ? (LUT)1 - inv : a[k] * inv;
 #pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const LUT pj = __shfl_sync(kFull, a[j], p);
-      if (lane != p) a[j] -= f * pj;
-    }
+    for (int j = 0; j < n; ++j)
+      if (j != k) a[j] = fma(-gi, pr[j], a[j]);
+    a[k] = (lane == p) ? inv : -gi;
   }
   if (row) {
 #pragma unroll
@@ -760,8 +778,14 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
 // Newton-matrix inverse of the cells of the setup list, one warp per cell:
 // Gauss-Jordan inverse of D (I - gamma J) D^-1 with D = diag(ewt) (FP32) or
 // of I - gamma J (FP64), written column-major into the cell record.
+// Minimum resident CTAs per SM requested for the inversion kernel (bounds
+// its registers per thread).
+#ifndef B200_GJ_MIN_CTAS
+#define B200_GJ_MIN_CTAS 4
+#endif
+
 template <int NS, typename LUT, int CPL>
-__global__ void __launch_bounds__(128) rk_gj(RoundsParams R) {
+__global__ void __launch_bounds__(128, B200_GJ_MIN_CTAS) rk_gj(RoundsParams R) {
   constexpr int n = NS + 1;
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
