@@ -439,8 +439,6 @@ def run_b200(args, rank, world, local_rank):
     for k in ("start", "rhs", "ctrl", "jac", "gj", "ctrl_setup"):
         v = prof[k]
         b = perfmodel.kernel_bytes(k, N) * v["cells"]
-        if k == "jac":
-            b += perfmodel.jac_refresh_bytes(N) * counters["nje"]
         kernels[k] = dict(v, share=v["ms"] / tot_ms if tot_ms else None,
                           algorithmic_gbs=(b / (v["ms"] * 1e-3) / 1e9) if v["ms"] else None, bytes=b)
     # dominant kernel: rk_ctrl (both of its launches per round)

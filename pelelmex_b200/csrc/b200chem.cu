@@ -413,40 +413,54 @@ int launch_kernel(b200chem_reactor* h, int lut, int what, int prof_kind, const R
   return 0;
 }
 
-int enqueue_round(b200chem_reactor* h, int lut, RoundsParams R, const RoundsGrids& G, int* list_in, int* cnt_in,
-                  int* list_out, int* cnt_out, int* list_setup, int* cnt_setup, cudaStream_t st) {
-  R.list_in = list_in;
-  R.cnt_in = cnt_in;
-  R.list_out = list_out;
-  R.cnt_out = cnt_out;
-  R.list_setup = list_setup;
-  R.cnt_setup = cnt_setup;
-  int err = launch_kernel(h, lut, kRoundsRhs, B200CHEM_PROF_RHS, R, G, 0, cnt_in, 0, st);
+// The slot lists of one chunk: A and B (cells needing a right-hand side,
+// swapped every round), S (cells needing a Newton-matrix setup) and its
+// subset SJ (setups that recompute the Jacobian).
+struct RoundLists {
+  int* lst[2];
+  int* cnt[2];
+  int* setup;
+  int* cnt_setup;
+  int* jac;
+  int* cnt_jac;
+};
+
+int enqueue_round(b200chem_reactor* h, int lut, RoundsParams R, const RoundsGrids& G, const RoundLists& Ls, int cur,
+                  cudaStream_t st) {
+  R.list_in = Ls.lst[cur];
+  R.cnt_in = Ls.cnt[cur];
+  R.list_out = Ls.lst[1 - cur];
+  R.cnt_out = Ls.cnt[1 - cur];
+  R.list_setup = Ls.setup;
+  R.cnt_setup = Ls.cnt_setup;
+  R.list_jac = Ls.jac;
+  R.cnt_jac = Ls.cnt_jac;
+  int err = launch_kernel(h, lut, kRoundsRhs, B200CHEM_PROF_RHS, R, G, 0, R.cnt_in, 0, st);
   if (err) return err;
-  CK(cudaMemsetAsync(cnt_out, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(cnt_setup, 0, sizeof(int), st));
-  if ((err = launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL, R, G, 1, cnt_in, 0, st))) return err;
-  R.list_in = list_setup;
-  R.cnt_in = cnt_setup;
-  if ((err = launch_kernel(h, lut, kRoundsJac, B200CHEM_PROF_JAC, R, G, 0, cnt_setup, 0, st))) return err;
-  if ((err = launch_kernel(h, lut, kRoundsGj, B200CHEM_PROF_GJ, R, G, 0, cnt_setup, 0, st))) return err;
+  CK(cudaMemsetAsync(R.cnt_out, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(Ls.cnt_setup, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(Ls.cnt_jac, 0, sizeof(int), st));
+  if ((err = launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL, R, G, 1, R.cnt_in, 0, st))) return err;
+  R.list_in = Ls.jac;
+  R.cnt_in = Ls.cnt_jac;
+  if ((err = launch_kernel(h, lut, kRoundsJac, B200CHEM_PROF_JAC, R, G, 0, Ls.cnt_jac, 0, st))) return err;
+  R.list_in = Ls.setup;
+  R.cnt_in = Ls.cnt_setup;
+  if ((err = launch_kernel(h, lut, kRoundsGj, B200CHEM_PROF_GJ, R, G, 0, Ls.cnt_setup, 0, st))) return err;
   // cells coming back from a setup always ask for a right-hand side next
-  return launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL_SETUP, R, G, 0, cnt_setup, 0, st);
+  return launch_kernel(h, lut, kRoundsCtrl, B200CHEM_PROF_CTRL_SETUP, R, G, 0, Ls.cnt_setup, 0, st);
 }
 
 // Captures `rounds` rounds (an even number: the two slot lists swap roles
 // every round, so the graph starts and ends on list A) into h->rgraph,
 // updating the executable graph in place when only kernel parameters
 // changed.
-int capture_rounds(b200chem_reactor* h, int lut, const RoundsParams& R, const RoundsGrids& G, int rounds, int* lst[2],
-                   int* cnt[2], int* listS, int* cntS) {
+int capture_rounds(b200chem_reactor* h, int lut, const RoundsParams& R, const RoundsGrids& G, int rounds,
+                   const RoundLists& Ls) {
   if (!h->cap_stream) CK(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
   CK(cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
   int err = 0;
-  for (int r = 0; r < rounds && !err; ++r) {
-    const int cur = r & 1;
-    err = enqueue_round(h, lut, R, G, lst[cur], cnt[cur], lst[1 - cur], cnt[1 - cur], listS, cntS, h->cap_stream);
-  }
+  for (int r = 0; r < rounds && !err; ++r) err = enqueue_round(h, lut, R, G, Ls, r & 1, h->cap_stream);
   cudaGraph_t g = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(h->cap_stream, &g);
   if (err || ce != cudaSuccess) {
@@ -520,15 +534,20 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
   R.P = P;
   R.SL = SL;
   R.S = rounds_carve(h->d_rounds, cap, h->N, lut);
-  // the three slot lists follow the cell records
+  // the four slot lists follow the cell records
   const size_t rec_bytes = (size_t)R.S.L.stride * cap;
-  if (rec_bytes + 12ull * cap > h->rounds_bytes)
+  if (rec_bytes + 16ull * cap > h->rounds_bytes)
     return set_err(B200CHEM_ECUDA, "round-integrator state layout overflows its buffer");
   int* lists = reinterpret_cast<int*>(static_cast<unsigned char*>(h->d_rounds) + rec_bytes);
-  int* lst[2] = {lists, lists + cap};
-  int* listS = lists + 2 * cap;
-  int* cnt[2] = {h->d_rcnt, h->d_rcnt + 1};
-  int* cntS = h->d_rcnt + 2;
+  RoundLists Ls;
+  Ls.lst[0] = lists;
+  Ls.lst[1] = lists + cap;
+  Ls.setup = lists + 2 * cap;
+  Ls.jac = lists + 3 * cap;
+  Ls.cnt[0] = h->d_rcnt;
+  Ls.cnt[1] = h->d_rcnt + 1;
+  Ls.cnt_setup = h->d_rcnt + 2;
+  Ls.cnt_jac = h->d_rcnt + 3;
   R.wscratch = static_cast<unsigned char*>(h->d_rwarp);
   // right-hand-side form: generated mechanism code, the constant bank or the
   // global tables
@@ -542,15 +561,17 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
     CK(cudaMemsetAsync(h->d_rcnt, 0, 4 * sizeof(int), st));
     R.list_in = nullptr;
     R.cnt_in = nullptr;
-    R.list_out = lst[0];
-    R.cnt_out = cnt[0];
-    R.list_setup = listS;
-    R.cnt_setup = cntS;
+    R.list_out = Ls.lst[0];
+    R.cnt_out = Ls.cnt[0];
+    R.list_setup = Ls.setup;
+    R.cnt_setup = Ls.cnt_setup;
+    R.list_jac = Ls.jac;
+    R.cnt_jac = Ls.cnt_jac;
     err = launch_kernel(h, lut, kRoundsStart, B200CHEM_PROF_START, R, G, 0, nullptr, R.nchunk, st);
     if (err) return err;
     h->launches++;
     if (graph) {
-      err = capture_rounds(h, lut, R, G, per_check, lst, cnt, listS, cntS);
+      err = capture_rounds(h, lut, R, G, per_check, Ls);
       if (err) return err;
     }
     for (long long round = 0;; round += per_check) {
@@ -559,14 +580,13 @@ int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
         CK(cudaGraphLaunch(h->rgraph, st));
       } else {
         for (int r = 0; r < per_check; ++r) {
-          const int cur = r & 1;
-          err = enqueue_round(h, lut, R, G, lst[cur], cnt[cur], lst[1 - cur], cnt[1 - cur], listS, cntS, st);
+          err = enqueue_round(h, lut, R, G, Ls, r & 1, st);
           if (err) return err;
         }
       }
       h->launches += 5LL * per_check;
       // per_check is even: the live cells are back in list A
-      CK(cudaMemcpyAsync(h->h_rcnt, cnt[0], sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(h->h_rcnt, Ls.cnt[0], sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       if (*h->h_rcnt == 0) break;
     }

@@ -43,7 +43,9 @@ enum Label : int {
 };
 
 // What the cell needs next.
-enum Need : int { kNeedRhs = 0, kNeedSetup = 1, kDone = 2 };
+// kNeedSetupJac: a setup whose Jacobian is stale (CVODE's jbad rule) and is
+// recomputed first; kNeedSetup: a setup that reuses the stored Jacobian.
+enum Need : int { kNeedRhs = 0, kNeedSetup = 1, kDone = 2, kNeedSetupJac = 3 };
 
 // Step-control record of one cell (doubles first, then ints), padded to a
 // multiple of 16 bytes so that it moves as 16-byte vectors.
@@ -536,7 +538,8 @@ __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, cons
 
 // Advance the cell from resume point `lab` until it needs a right-hand side
 // at v.yev (returns kNeedRhs with c.label set to the label that consumes it),
-// a setup (kNeedSetup), or is finished (kDone, *status set).
+// a setup (kNeedSetup, or kNeedSetupJac with a Jacobian refresh), or is
+// finished (kDone, *status set).
 template <int n, int G, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
                                          const double* J, const LUT* A, int gl, unsigned gm, int* status) {
@@ -666,6 +669,18 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         if (c.callSetup) {
           c.setup_conv = c.jbad ? kFailBadJ : c.convfail;
           c.label = kLAfterSetup;
+          // CVODE's jbad rule: recompute J on the first step, every msbj
+          // steps, or after a convergence failure (with a stale J, or with
+          // gamma little changed)
+          const double dgamma = fabs(c.gamma / c.gammap - 1.0);
+          const bool jbad = (c.cnt.nst == 0) || (c.cnt.nst >= c.nstlj + kMSBJ) ||
+                            (c.setup_conv == kFailBadJ && dgamma < kDGMAX_JBAD) || (c.setup_conv == kFailOther);
+          c.jcur = jbad ? 1 : 0;
+          if (jbad) {
+            c.cnt.nje++;
+            c.nstlj = c.cnt.nst;
+            return kNeedSetupJac;
+          }
           return kNeedSetup;
         }
         c.mnewt = 0;

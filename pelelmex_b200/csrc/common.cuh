@@ -134,6 +134,8 @@ struct RoundsParams {
   int* cnt_out;
   int* list_setup;   // cells that need a Newton-matrix setup this round
   int* cnt_setup;
+  int* list_jac;     // the subset of list_setup whose Jacobian is recomputed
+  int* cnt_jac;
   unsigned char* wscratch;  // [setup warps][SL.gbytes_per_warp]
   int const_mech;           // 1: the packed table is in the constant bank
   int gen_mech;             // 1: the mechanism has a generated right-hand side

@@ -504,7 +504,8 @@ __global__ void __launch_bounds__(128, B200_CTRL_MIN_CTAS) rk_ctrl(RoundsParams 
     }
     const bool lead = live && gl == 0;
     warp_append(lead && need == kNeedRhs, slot, R.list_out, R.cnt_out);
-    warp_append(lead && need == kNeedSetup, slot, R.list_setup, R.cnt_setup);
+    warp_append(lead && (need == kNeedSetup || need == kNeedSetupJac), slot, R.list_setup, R.cnt_setup);
+    warp_append(lead && need == kNeedSetupJac, slot, R.list_jac, R.cnt_jac);
     warp_stats(P.stats, lead && need == kDone, status != 0, false, c.cnt);
   }
 }
@@ -748,42 +749,30 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
   for (long long idx = gw; idx < cnt; idx += nwarps) {
     const int slot = R.list_in[idx];
     unsigned char* rec = rec_of(R.S, slot);
-    RCell* cp = reinterpret_cast<RCell*>(rec);
-    const int nst = cp->cnt.nst, nstlj = cp->nstlj, sconv = cp->setup_conv;
-    const double dgamma = fabs(cp->gamma / cp->gammap - 1.0);
-    const bool jbad = (nst == 0) || (nst >= nstlj + kMSBJ) || (sconv == kFailBadJ && dgamma < kDGMAX_JBAD) ||
-                      (sconv == kFailOther);
-    if (jbad) {
-      const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
-      Vec<CPL> y, fy;
+    // the control kernel chose these cells by CVODE's jbad rule and already
+    // counted the refresh
+    const RVec<n> v{reinterpret_cast<double*>(rec + RL.off_vec)};
+    Vec<CPL> y, fy;
 #pragma unroll
-      for (int cc = 0; cc < CPL; ++cc) {
-        const int i = lane + 32 * cc;
-        y.v[cc] = (i < n) ? v.yev(i) : 0.0;
-        fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
-      }
-      warp_jac<CPL>(s_mech, ms, Js, us, y, fy, reinterpret_cast<double*>(rec + RL.off_j), RL.ldj, lane);
-      if (lane == 0) {
-        cp->cnt.nje++;
-        cp->nstlj = nst;
-        cp->jcur = 1;
-      }
-    } else if (lane == 0) {
-      cp->jcur = 0;
+    for (int cc = 0; cc < CPL; ++cc) {
+      const int i = lane + 32 * cc;
+      y.v[cc] = (i < n) ? v.yev(i) : 0.0;
+      fy.v[cc] = (i < n) ? v.ftemp(i) : 0.0;
     }
+    warp_jac<CPL>(s_mech, ms, Js, us, y, fy, reinterpret_cast<double*>(rec + RL.off_j), RL.ldj, lane);
     __syncwarp();
   }
 }
 
-// Newton-matrix inverse of the cells of the setup list, one warp per cell:
-// Gauss-Jordan inverse of D (I - gamma J) D^-1 with D = diag(ewt) (FP32) or
-// of I - gamma J (FP64), written column-major into the cell record.
 // Minimum resident CTAs per SM requested for the inversion kernel (bounds
 // its registers per thread).
 #ifndef B200_GJ_MIN_CTAS
 #define B200_GJ_MIN_CTAS 4
 #endif
 
+// Newton-matrix inverse of the cells of the setup list, one warp per cell:
+// Gauss-Jordan inverse of D (I - gamma J) D^-1 with D = diag(ewt) (FP32) or
+// of I - gamma J (FP64), written column-major into the cell record.
 template <int NS, typename LUT, int CPL>
 __global__ void __launch_bounds__(128, B200_GJ_MIN_CTAS) rk_gj(RoundsParams R) {
   constexpr int n = NS + 1;
@@ -937,7 +926,7 @@ RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes) {
 }
 
 long long rounds_state_bytes_per_cell(int N, int lut_bytes) {
-  return rounds_record_layout(N + 1, lut_bytes).stride + 4LL * 3;  // record + three slot lists
+  return rounds_record_layout(N + 1, lut_bytes).stride + 4LL * 4;  // record + four slot lists
 }
 
 RState rounds_carve(void* base, long long cap, int N, int lut_bytes) {

@@ -102,15 +102,15 @@ RCELL_BYTES = 448  # step-control record of the round-based integrator
 def kernel_bytes(kind: str, n_species: int, lut_bytes: int = 4) -> float:
     """Algorithmic HBM bytes ONE processed cell costs in a kernel of the
     round-based integrator (bytes the step of the algorithm must read and
-    write, each once; the Jacobian kind's refresh is counted separately by
-    jac_refresh_bytes because only the cells whose Jacobian is stale redo it):
+    write, each once):
 
     * rhs: list slot, read y and the forcing (2n), write f (n)
     * ctrl / ctrl_setup (one Newton iteration): the step-control record read
       and written, read zn[1], acor, ftemp, f, ewt, scaling (6n) and write
       acor (n), read the FP64 Jacobian (n^2) for the refinement residual and
       the inverse (n^2 at lut_bytes)
-    * jac: list slot and the step counters deciding the refresh
+    * jac (only the setups whose Jacobian is stale reach it): list slot,
+      read y and f (2n), write J (n^2)
     * gj: list slot and gamma, read J (n^2) and ewt (n), write the scaling
       (n) and the inverse (n^2 at lut_bytes)
     """
@@ -120,7 +120,7 @@ def kernel_bytes(kind: str, n_species: int, lut_bytes: int = 4) -> float:
     if kind in ("ctrl", "ctrl_setup"):
         return 4 + 2 * RCELL_BYTES + 8 * 7 * n + 8 * n * n + lut_bytes * n * n
     if kind == "jac":
-        return 4 + 40
+        return 4 + jac_refresh_bytes(n_species)
     if kind == "gj":
         return 4 + 16 + 8 * n * n + 8 * 2 * n + lut_bytes * n * n
     if kind == "start":
