@@ -338,7 +338,7 @@ class HybridReactor:
             if fctCount is not None:
                 fctCount.index_copy_(0, rej, fc + 2.0)
         counts = torch.bincount((-accept).clamp_min(0), minlength=6).tolist()
-        self.last = {"cells": nc, "rejected": nrej, "accepted_fraction": 1.0 - nrej / nc,
+        self.last = {"cells": nc, "rejected": nrej, "accepted_fraction": 1.0 - nrej / nc, "accepted": accept == 1,
                      "rejected_by": {"mass": counts[1], "elements": counts[2], "energy": counts[3],
                                      "residual": counts[4], "change": counts[5]}}
         return nrej
