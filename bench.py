@@ -35,6 +35,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from pelelmex_b200 import sharding  # noqa: E402
+
 METRIC = "cells/s per chem step (drm19 128^3) at ≤1e-4 T err: hybrid vs plain GPU BDF"
 UNIT = "cells/s"
 MECH = "synth_ch4_21"
@@ -305,10 +307,7 @@ def run_b200(args, rank, world, local_rank):
     barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms = sum(step_ms) / len(step_ms)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = sharding.step_time_max(ms, dev)
     value = world * nc / (ms * 1e-3)
     plain = {"value": value, "unit": UNIT, "ms_per_step": ms, "step_ms": step_ms}
 
@@ -348,10 +347,7 @@ def run_b200(args, rank, world, local_rank):
         barrier()
         hstep = [a.elapsed_time(b) for a, b in hev]
         hms = sum(hstep) / len(hstep)
-        if world > 1:
-            t = torch.tensor([hms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            hms = float(t.item())
+        hms = sharding.step_time_max(hms, dev)
         # the tensor-core forward pass alone (4 GEMMs over every cell)
         nrows = (nc + 127) // 128 * 128
         x = nets[0].features(r, base["rhoY"], base["T"], field.dt, nrows)
@@ -420,10 +416,7 @@ def run_b200(args, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1) / args.steps
-        if world > 1:
-            t = torch.tensor([ems], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = sharding.step_time_max(ems, dev)
         e2e = {"value": world * nc / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
 
@@ -515,14 +508,14 @@ def run_dodecane(args, rank, world, local_rank):
     N = mech.n_species
     if args.workload == "c12_boxes":
         boxes = workloads.c12_boxes(mech, dt=args.dt)
-        mine = boxes[rank::world]
+        mine = sharding.shard_boxes(boxes, rank, world)
         total = sum(f.ncells for _, _, f in boxes)
         wl = (f"c12_boxes: {len(boxes)} dodecane boxes (edges 16/32/64, half cold 300-600 K, half igniting "
               f"900-1400 K, phi 0.5-2), {total} cells, one react launch per box list")
         flat = [f for _, _, f in mine]
     else:
         n_all = args.edge ** 3
-        idx = np.arange(rank, n_all, world, dtype=np.int64)
+        idx = sharding.shard_cells(n_all, rank, world)
         flat = [workloads.c12_flame_grf(mech, edge=args.edge, dt=args.dt, cells=idx)]
         total = n_all
         wl = f"c12_grf: dodecane random-field flame {args.edge}^3 (T 300-2400 K, Z 0-1), {total} cells"
@@ -617,10 +610,8 @@ def run_dodecane(args, rank, world, local_rank):
     launches = r.kernel_launches() - l0
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms = sum(step_ms) / len(step_ms)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = sharding.step_time_max(ms, dev)
+    counters = sharding.counters_sum(counters, dev)
     if rank != 0:
         r.close()
         return
@@ -672,11 +663,12 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.dt is None:
         args.dt = 5e-6 if args.workload == "c12_grf" else 1e-6
-    if args.workload != "flame_ch4":
-        run_dodecane(args, rank, world, local_rank)
-        return
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        # the CPU reference runs on rank 0 alone; the other ranks exit
+        if args.workload != "flame_ch4":
+            run_dodecane(args, rank, world, local_rank)
+        else:
+            run_reference(args, rank, world)
         return
     if world > 1:
         import datetime
@@ -686,7 +678,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_b200(args, rank, world, local_rank)
+        if args.workload != "flame_ch4":
+            run_dodecane(args, rank, world, local_rank)
+        else:
+            run_b200(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
