@@ -443,6 +443,65 @@ __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// One cell of the control kernel, G lanes per cell: resume the CVODE state
+// machine (after_rhs: consuming the f just evaluated, counted in nfe;
+// otherwise coming back from a setup), write the outputs of a finished cell,
+// and append the cell to the list of its next need.  Every lane of the warp
+// calls it (the appends are warp-collective); `live` marks the groups with a
+// cell.
+template <int NS, int G, typename LUT>
+__device__ __forceinline__ void ctrl_cell(const RoundsParams& R, bool live, int slot, bool after_rhs, int gl,
+                                          unsigned gm, int idx_next) {
+  constexpr int n = NS + 1;
+  const ReactParams& P = R.P;
+  int need = kDone, status = 0;
+  RCell c;
+  if (live) {
+    unsigned char* rec = rec_of(R.S, slot);
+    if (B200_CTRL_PREFETCH >= 1 && gl == 0)
+      l2_prefetch(rec + R.S.L.off_vec, (uint32_t)(R.S.L.stride - R.S.L.off_vec));
+    if (B200_CTRL_PREFETCH >= 2 && gl == 0 && idx_next >= 0)
+      l2_prefetch(rec_of(R.S, R.list_in[idx_next]), (uint32_t)R.S.L.off_j);
+    load_cell(c, rec);
+    if (after_rhs) c.cnt.nfe++;
+    const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
+    need = r_advance<n, G, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
+                                reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status);
+    __syncwarp(gm);
+    if (gl == 0) store_cell(c, rec);
+    if (need == kDone) {
+      const long long cell = R.chunk0 + slot;
+      const CellLoc L = locate(P, cell);
+      const DevBox& bx = *L.bx;
+      if (status == 0) {
+        // y(dt) from the Nordsieck array (Horner in s = (dt - tn) / h)
+        const double s = (P.dt - c.tn) / c.h;
+        double* yp = elem(bx.rhoY, L.i, L.j, L.k);
+        const int q = c.q;
+        each<n, G>(gl, [&](int k) {
+          double y = v.zn(q, k);
+          for (int jj = q - 1; jj >= 0; --jj) y = v.zn(jj, k) + s * y;
+          if (k < NS) yp[k * bx.rhoY.ns] = y;
+          else *elem(bx.T, L.i, L.j, L.k) = y;
+        });
+        if (gl == 0) {
+          double* hp = elem(bx.rhoH, L.i, L.j, L.k);
+          *hp = *hp + P.dt * v.F(NS);
+        }
+      }
+      if (gl == 0) {
+        if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
+        if (P.status) P.status[cell] = status;
+      }
+    }
+  }
+  const bool lead = live && gl == 0;
+  warp_append(lead && need == kNeedRhs, slot, R.list_out, R.cnt_out);
+  warp_append(lead && (need == kNeedSetup || need == kNeedSetupJac), slot, R.list_setup, R.cnt_setup);
+  warp_append(lead && need == kNeedSetupJac, slot, R.list_jac, R.cnt_jac);
+  warp_stats(P.stats, lead && need == kDone, status != 0, false, c.cnt);
+}
+
 // Resume the cells of list_in, G lanes per cell.  after_rhs: each consumes
 // the f just evaluated (counted in nfe); otherwise they come back from a
 // setup.
@@ -451,7 +510,6 @@ __global__ void __launch_bounds__(128, B200_CTRL_MIN_CTAS) rk_ctrl(RoundsParams 
   constexpr int n = NS + 1;
   constexpr int G = ctrl_group(n);
   constexpr int GPW = 32 / G;  // cells per warp
-  const ReactParams& P = R.P;
   const int cnt = *R.cnt_in;
   const int lane = threadIdx.x & 31, gl = lane % G, gi = lane / G;
   const unsigned gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gi * G));
@@ -460,53 +518,8 @@ __global__ void __launch_bounds__(128, B200_CTRL_MIN_CTAS) rk_ctrl(RoundsParams 
   for (int base = wid * GPW; base < cnt; base += nw * GPW) {
     const int idx = base + gi;
     const bool live = idx < cnt;
-    int slot = 0, need = kDone, status = 0;
-    RCell c;
-    if (live) {
-      slot = R.list_in[idx];
-      unsigned char* rec = rec_of(R.S, slot);
-      if (B200_CTRL_PREFETCH >= 1 && gl == 0)
-        l2_prefetch(rec + R.S.L.off_vec, (uint32_t)(R.S.L.stride - R.S.L.off_vec));
-      if (B200_CTRL_PREFETCH >= 2 && gl == 0 && idx + nw * GPW < cnt)
-        l2_prefetch(rec_of(R.S, R.list_in[idx + nw * GPW]), (uint32_t)R.S.L.off_j);
-      load_cell(c, rec);
-      if (after_rhs) c.cnt.nfe++;
-      const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
-      need = r_advance<n, G, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
-                                  reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status);
-      __syncwarp(gm);
-      if (gl == 0) store_cell(c, rec);
-      if (need == kDone) {
-        const long long cell = R.chunk0 + slot;
-        const CellLoc L = locate(P, cell);
-        const DevBox& bx = *L.bx;
-        if (status == 0) {
-          // y(dt) from the Nordsieck array (Horner in s = (dt - tn) / h)
-          const double s = (P.dt - c.tn) / c.h;
-          double* yp = elem(bx.rhoY, L.i, L.j, L.k);
-          const int q = c.q;
-          each<n, G>(gl, [&](int k) {
-            double y = v.zn(q, k);
-            for (int jj = q - 1; jj >= 0; --jj) y = v.zn(jj, k) + s * y;
-            if (k < NS) yp[k * bx.rhoY.ns] = y;
-            else *elem(bx.T, L.i, L.j, L.k) = y;
-          });
-          if (gl == 0) {
-            double* hp = elem(bx.rhoH, L.i, L.j, L.k);
-            *hp = *hp + P.dt * v.F(NS);
-          }
-        }
-        if (gl == 0) {
-          if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
-          if (P.status) P.status[cell] = status;
-        }
-      }
-    }
-    const bool lead = live && gl == 0;
-    warp_append(lead && need == kNeedRhs, slot, R.list_out, R.cnt_out);
-    warp_append(lead && (need == kNeedSetup || need == kNeedSetupJac), slot, R.list_setup, R.cnt_setup);
-    warp_append(lead && need == kNeedSetupJac, slot, R.list_jac, R.cnt_jac);
-    warp_stats(P.stats, lead && need == kDone, status != 0, false, c.cnt);
+    const int nxt = idx + nw * GPW;
+    ctrl_cell<NS, G, LUT>(R, live, live ? R.list_in[idx] : 0, after_rhs != 0, gl, gm, nxt < cnt ? nxt : -1);
   }
 }
 
