@@ -379,7 +379,9 @@ def run_b200(args, rank, world, local_rank):
                                   "bf16_peak_tflops": bf16_peak,
                                   "frac": (mlp_flops / (mlp_ms * 1e-3) / 1e12 / bf16_peak) if bf16_peak else None,
                                   "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops)"}}
-        if terr <= 1e-4:
+        # the headline is the faster of the two integrators that meets the
+        # 1e-4 temperature bar (the plain BDF always does: it is the reference)
+        if terr <= 1e-4 and hybrid["value"] > value:
             value = hybrid["value"]
 
     # end to end through the public API from pinned host buffers
