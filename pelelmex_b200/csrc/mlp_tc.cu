@@ -415,7 +415,10 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_bf16_tc(GemmArgs g) {
 // are 128 bytes apart, its stride byte offset).  Barriers: full / empty per
 // stage, acc_full / acc_empty per accumulator; every wait is bounded and a
 // timeout stops all roles.
-constexpr int kEpiPerQuarter = 2;                        // epilogue warps per TMEM lane quarter
+#ifndef B200_EPI_PER_QUARTER
+#define B200_EPI_PER_QUARTER 2
+#endif
+constexpr int kEpiPerQuarter = B200_EPI_PER_QUARTER;     // epilogue warps per TMEM lane quarter
 constexpr int kEpiWarps = 4 * kEpiPerQuarter;
 constexpr int kWsThreads = 64 + 32 * kEpiWarps;
 constexpr int kMaxStages = 8;
