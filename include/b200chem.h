@@ -196,6 +196,33 @@ int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* e
                                 const int32_t* mask, int64_t ncells, double* dt_react, double* time,
                                 void* stream, int32_t* cell_status, b200chem_stats* stats);
 
+/* ------------------------------------------------ advanceChemistry body
+ * One box of PeleLM::advanceChemistry(lev, dt, extForcing)
+ * (Source/PeleLMeX_Reactions.cpp:31-175) around react, in MKS units like
+ * the caller's MultiFabs: new <- old converted to CGS (:68-79), react with
+ * dt_react = dt and time = 0 (:97-108), the new state and the forcing back to
+ * MKS (:111-120), and the reaction term I_R = -(rhoY_old - rhoY_new) / dt -
+ * extF_rhoY (:153-160).  extF_rhoY / extF_rhoH are scaled in place and back,
+ * as the reference does.  All boxes of the list go through one prologue
+ * launch, one react and one epilogue launch. */
+typedef struct b200chem_chem_box {
+  int32_t lo[3], hi[3];
+  b200chem_array4 rhoY_old;  /* N comps, in,  kg/m^3                      */
+  b200chem_array4 rhoH_old;  /* 1 comp,  in,  J/m^3                       */
+  b200chem_array4 T_old;     /* 1 comp,  in,  K                           */
+  b200chem_array4 rhoY_new;  /* N comps, out, kg/m^3                      */
+  b200chem_array4 rhoH_new;  /* 1 comp,  out, J/m^3                       */
+  b200chem_array4 T_new;     /* 1 comp,  out, K                           */
+  b200chem_array4 extF_rhoY; /* N comps, in (scaled and restored), kg/m^3/s */
+  b200chem_array4 extF_rhoH; /* 1 comp,  in (scaled and restored), J/m^3/s  */
+  b200chem_array4 fctCount;  /* 1 comp,  out (p may be NULL)              */
+  b200chem_iarray4 mask;     /* 1 comp,  in, 0 = skip (p may be NULL)     */
+  b200chem_array4 I_R;       /* N comps, out, kg/m^3/s (p may be NULL)    */
+} b200chem_chem_box;
+
+int b200chem_advance_chemistry(b200chem_handle h, const b200chem_chem_box* boxes, int32_t nbox, double dt,
+                               void* stream, int32_t* cell_status, b200chem_stats* stats);
+
 /* ReactorBase::close (Source/PeleLMeX.cpp:26). */
 int b200chem_destroy(b200chem_handle h);
 

@@ -34,6 +34,13 @@ class BoxView(ctypes.Structure):
                 ("T", Array4), ("rhoH", Array4), ("extF_rhoH", Array4), ("fctCount", Array4), ("mask", Array4)]
 
 
+class ChemBox(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3), ("rhoY_old", Array4), ("rhoH_old", Array4),
+                ("T_old", Array4), ("rhoY_new", Array4), ("rhoH_new", Array4), ("T_new", Array4),
+                ("extF_rhoY", Array4), ("extF_rhoH", Array4), ("fctCount", Array4), ("mask", Array4),
+                ("I_R", Array4)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("n_cells", ctypes.c_int64), ("n_masked", ctypes.c_int64), ("n_failed", ctypes.c_int64),
                 ("nst", ctypes.c_int64), ("nfe", ctypes.c_int64), ("nje", ctypes.c_int64), ("nlu", ctypes.c_int64),
@@ -118,6 +125,9 @@ def load(path: os.PathLike | None = None):
     L.b200chem_autotune.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int64,
                                     ctypes.c_double, ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(Tuning),
                                     ctypes.POINTER(ctypes.c_double)]
+    L.b200chem_advance_chemistry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChemBox), ctypes.c_int32,
+                                             ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.b200chem_advance_chemistry.restype = ctypes.c_int
     L.b200chem_profile_begin.argtypes = [ctypes.c_void_p]
     L.b200chem_profile_end.argtypes = [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]
     for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune", "b200chem_profile_begin",

@@ -217,6 +217,11 @@ struct b200chem_reactor {
   cudaStream_t cap_stream = nullptr;  // private stream the round graph is captured on
   cudaGraphExec_t rgraph = nullptr;   // executable graph of rounds_per_check rounds
   int rgraph_rounds = 0;              // rounds in rgraph
+  void* d_cboxes = nullptr;           // advanceChemistry box descriptors (device, pinned staging)
+  void* h_cboxes = nullptr;
+  size_t cboxes_bytes = 0;
+  bool cboxes_pending = false;
+  cudaEvent_t cbox_ev = nullptr;
   // per-kernel profile of the round integrator (b200chem_profile_begin/end)
   struct ProfRec {
     int kind;
@@ -982,6 +987,81 @@ int b200chem_react(b200chem_handle h, const b200chem_box_view* views, int32_t nb
   return err;
 }
 
+int b200chem_advance_chemistry(b200chem_handle h, const b200chem_chem_box* cboxes, int32_t nbox, double dt,
+                               void* stream, int32_t* cell_status, b200chem_stats* stats) {
+  if (!h || (!cboxes && nbox > 0) || nbox < 0) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!(dt > 0.0)) return set_err(B200CHEM_EINVAL, "dt must be positive");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::vector<ChemBoxDev> cb(nbox);
+  std::vector<b200chem_box_view> views(nbox);
+  long long total = 0;
+  for (int b = 0; b < nbox; ++b) {
+    const b200chem_chem_box& x = cboxes[b];
+    if (!x.rhoY_old.p || !x.rhoH_old.p || !x.T_old.p || !x.rhoY_new.p || !x.rhoH_new.p || !x.T_new.p ||
+        !x.extF_rhoY.p || !x.extF_rhoH.p)
+      return set_err(B200CHEM_EINVAL, "box %d: null state array", b);
+    ChemBoxDev& d = cb[b];
+    d.lo0 = x.lo[0];
+    d.lo1 = x.lo[1];
+    d.lo2 = x.lo[2];
+    d.nx = x.hi[0] - x.lo[0] + 1;
+    d.ny = x.hi[1] - x.lo[1] + 1;
+    d.nz = x.hi[2] - x.lo[2] + 1;
+    if (d.nx < 1 || d.ny < 1 || d.nz < 1) return set_err(B200CHEM_EINVAL, "box %d is empty or inverted", b);
+    d.off = total;
+    total += (long long)d.nx * d.ny * d.nz;
+    d.rY_o = to_dev(x.rhoY_old);
+    d.rH_o = to_dev(x.rhoH_old);
+    d.T_o = to_dev(x.T_old);
+    d.rY_n = to_dev(x.rhoY_new);
+    d.rH_n = to_dev(x.rhoH_new);
+    d.T_n = to_dev(x.T_new);
+    d.fY = to_dev(x.extF_rhoY);
+    d.fH = to_dev(x.extF_rhoH);
+    d.IR = to_dev(x.I_R);
+    b200chem_box_view& v = views[b];
+    memcpy(v.lo, x.lo, sizeof(v.lo));
+    memcpy(v.hi, x.hi, sizeof(v.hi));
+    v.rhoY = x.rhoY_new;
+    v.extF_rhoY = x.extF_rhoY;
+    v.T = x.T_new;
+    v.rhoH = x.rhoH_new;
+    v.extF_rhoH = x.extF_rhoH;
+    v.fctCount = x.fctCount;
+    v.mask = x.mask;
+  }
+  if (total == 0) return 0;
+  // box descriptors: pinned staging, device copy (reused across calls)
+  const size_t bytes = sizeof(ChemBoxDev) * (size_t)nbox;
+  if (!h->cbox_ev) CK(cudaEventCreateWithFlags(&h->cbox_ev, cudaEventDisableTiming));
+  // the pinned staging buffer is reused once the previous call's copy from it is done
+  if (h->cboxes_pending) CK(cudaEventSynchronize(h->cbox_ev));
+  h->cboxes_pending = false;
+  if (bytes > h->cboxes_bytes) {
+    if (h->d_cboxes) cudaFree(h->d_cboxes);
+    if (h->h_cboxes) cudaFreeHost(h->h_cboxes);
+    h->d_cboxes = nullptr;
+    h->h_cboxes = nullptr;
+    h->cboxes_bytes = 0;
+    CK(cudaMalloc(&h->d_cboxes, bytes));
+    CK(cudaMallocHost(&h->h_cboxes, bytes));
+    h->cboxes_bytes = bytes;
+  }
+  memcpy(h->h_cboxes, cb.data(), bytes);
+  CK(cudaMemcpyAsync(h->d_cboxes, h->h_cboxes, bytes, cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(h->cbox_ev, st));
+  h->cboxes_pending = true;
+  CK(advance_chem_launch(0, static_cast<const ChemBoxDev*>(h->d_cboxes), nbox, total, h->N, 0.0, h->sm_count, st));
+  h->launches++;
+  double dt_react = dt, time = 0.0;
+  int err = b200chem_react(h, views.data(), nbox, &dt_react, &time, stream, cell_status, stats);
+  if (err && err != B200CHEM_EINTEGRATE) return err;
+  CK(advance_chem_launch(1, static_cast<const ChemBoxDev*>(h->d_cboxes), nbox, total, h->N, 1.0 / dt, h->sm_count,
+                         st));
+  h->launches++;
+  return err;
+}
+
 int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T, double* rhoH,
                         const double* extF_rhoH, double* fctCount, const int32_t* mask, int64_t ncells,
                         double* dt_react, double* time, void* stream, int32_t* cell_status, b200chem_stats* stats) {
@@ -1363,6 +1443,10 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
   if (h->h_cmech) cudaFreeHost(h->h_cmech);
   if (h->rgraph) cudaGraphExecDestroy(h->rgraph);
+  if (h->cboxes_pending) cudaEventSynchronize(h->cbox_ev);
+  if (h->cbox_ev) cudaEventDestroy(h->cbox_ev);
+  if (h->d_cboxes) cudaFree(h->d_cboxes);
+  if (h->h_cboxes) cudaFreeHost(h->h_cboxes);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->h_pcnt) cudaFreeHost(h->h_pcnt);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);

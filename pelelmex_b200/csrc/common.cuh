@@ -27,6 +27,17 @@ struct DevBox {
   DevIArr mask;
 };
 
+// One box of the advanceChemistry body (advance_chem.cu): old state,
+// new state, forcing and the reaction term, MKS.
+struct ChemBoxDev {
+  int lo0, lo1, lo2, nx, ny, nz;
+  long long off;
+  DevArr rY_o, rH_o, T_o, rY_n, rH_n, T_n, fY, fH, IR;
+};
+// phase 0: MKS -> CGS prologue; 1: CGS -> MKS epilogue and I_R
+cudaError_t advance_chem_launch(int phase, const ChemBoxDev* d_boxes, int nbox, long long total, int N,
+                                double dt_inv, int sm_count, cudaStream_t st);
+
 // stats slots in the scratch buffer (after the queue counter)
 enum { kStCells = 0, kStMasked, kStFailed, kStNst, kStNfe, kStNje, kStNlu, kStNetf, kStNcfn, kStMaxNfe,
        kStMaxNst, kStCount };

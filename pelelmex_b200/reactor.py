@@ -270,6 +270,35 @@ class ReactorB200:
             self._h, views, len(items), dtp, tp, st, sp, stp), dt_react, time, stream, status, stats,
             raise_on_failure)
 
+    def advance_chemistry(self, items, dt, stream=None, status=None, stats=False, raise_on_failure=True):
+        """PeleLM::advanceChemistry's box body (Source/PeleLMeX_Reactions.cpp:31-175) for a
+        list of boxes, MKS fabs: each item is (box, rhoY_old, rhoH_old, T_old, rhoY_new,
+        rhoH_new, T_new, extF_rhoY, extF_rhoH, fctCount, mask, I_R[, fab_lo]); fctCount,
+        mask and I_R may be None.  Returns stats (dict) when asked, else None."""
+        self._need()
+        boxes = (_lib.ChemBox * max(len(items), 1))()
+        for b, it in enumerate(items):
+            box = it[0]
+            flo = it[12] if len(it) > 12 and it[12] is not None else box.lo
+            x = boxes[b]
+            x.lo[:] = list(box.lo)
+            x.hi[:] = list(box.hi)
+            names = ("rhoY_old", "rhoH_old", "T_old", "rhoY_new", "rhoH_new", "T_new", "extF_rhoY", "extF_rhoH",
+                     "fctCount", "mask", "I_R")
+            for name, t in zip(names, it[1:12]):
+                setattr(x, name, array4(t, flo))
+            if it[1].shape[0] != self.N or it[4].shape[0] != self.N:
+                raise ValueError(f"rhoY has {it[1].shape[0]} components, mechanism has {self.N}")
+        st_obj = _lib.Stats()
+        code = _lib.load().b200chem_advance_chemistry(
+            self._h, boxes, len(items), float(dt), _stream_ptr(stream),
+            status.data_ptr() if status is not None else None, ctypes.byref(st_obj) if stats else None)
+        s = st_obj.as_dict() if stats else None
+        if code != 0 and (code != -4 or raise_on_failure):
+            raise ReactorError(f"advance_chemistry failed ({code}): {_lib.load().b200chem_last_error().decode()}",
+                               status=status, stats=s)
+        return s
+
     def react_flat(self, rhoY, extF_rhoY, T, rhoH, extF_rhoH, fctCount=None, mask=None, dt_react=1e-6,
                    time=0.0, stream=None, status=None, stats=False, raise_on_failure=True):
         """Flat form: rhoY/extF_rhoY are [N, ncells] CUDA tensors (component-major)."""
