@@ -320,6 +320,16 @@ int b200chem_inst_rr(b200chem_handle h, const double* rhoY_mks, const double* rh
 int b200chem_t_from_hy(b200chem_handle h, const double* rhoY_mks, const double* rhoH_mks,
                        double* T, int64_t ncells, void* stream);
 
+/* getHGivenT (Source/PeleLMeX_K.H:598-615): species enthalpies h_k(T) in
+ * J/kg, component-major Hi[k * ncells + c]. */
+int b200chem_h_given_t(b200chem_handle h, const double* T, double* Hi_mks, int64_t ncells, void* stream);
+
+/* getHeatRelease (Source/PeleLMeX_Reactions.cpp:477-506): heat release rate
+ * HRR = -sum_k h_k(T) I_R,k in W/m^3, from T and the reaction term I_R
+ * (kg/m^3/s, component-major, as b200chem_advance_chemistry writes it). */
+int b200chem_heat_release(b200chem_handle h, const double* T, const double* I_R_mks, double* HR_mks,
+                          int64_t ncells, void* stream);
+
 /* ------------------------------------------------------- surrogate MLP
  * No reference counterpart: the learned part of the reactor (a small MLP
  * predicting the state change over dt_react, with residual-gated fallback to

@@ -138,6 +138,10 @@ def load(path: os.PathLike | None = None):
         f.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, _f64p, ctypes.c_void_p]
     L.b200chem_inst_rr.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
     L.b200chem_t_from_hy.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
+    L.b200chem_h_given_t.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
+    L.b200chem_heat_release.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, ctypes.c_int64, ctypes.c_void_p]
+    L.b200chem_h_given_t.restype = ctypes.c_int
+    L.b200chem_heat_release.restype = ctypes.c_int
     for name in ("b200chem_set_typvals", "b200chem_react", "b200chem_react_flat", "b200chem_destroy",
                  "b200chem_eval_rhs", "b200chem_eval_jac", "b200chem_inst_rr", "b200chem_t_from_hy"):
         getattr(L, name).restype = ctypes.c_int

@@ -179,6 +179,29 @@ __global__ void __launch_bounds__(128) inst_rr_kernel(InstParams P) {
   }
 }
 
+// getHGivenT (Source/PeleLMeX_K.H:598-615) and getHeatRelease
+// (Source/PeleLMeX_Reactions.cpp:477-506), thread per cell: species
+// enthalpies h_k(T) (CEPTR's T2Hi, erg/g) converted to J/kg, and
+// HRR = -sum_k h_k I_R,k (the reference's accumulation order, one FMA per
+// species).  Component-major arrays of ncells.
+__global__ void thermo_hr_kernel(DevMech m, const double* __restrict__ T, const double* __restrict__ IR,
+                                 double* __restrict__ Hi, double* __restrict__ HR, long long ncells) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncells;
+       c += (long long)gridDim.x * blockDim.x) {
+    const double t = T[c];
+    const double lnT = log(t);
+    double hr = 0.0;
+    for (int k = 0; k < m.N; ++k) {
+      double cpR, hRT, sR, dcpR;
+      nasa7(m, k, t, lnT, cpR, hRT, sR, dcpR);
+      const double hk = hRT * kRu * t * __ldg(m.inv_mw + k) * 0.0001;  // erg/g -> J/kg
+      if (Hi) Hi[(long long)k * ncells + c] = hk;
+      if (HR) hr = fma(-hk, IR[(long long)k * ncells + c], hr);
+    }
+    if (HR) HR[c] = hr;
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ handle
@@ -1526,6 +1549,28 @@ int b200chem_inst_rr(b200chem_handle h, const double* rhoY_mks, const double* rh
 int b200chem_t_from_hy(b200chem_handle h, const double* rhoY_mks, const double* rhoH_mks, double* T, int64_t ncells,
                        void* stream) {
   return inst_launch(h, rhoY_mks, rhoH_mks, T, nullptr, ncells, stream);
+}
+
+static int thermo_launch(b200chem_handle h, const double* T, const double* IR, double* Hi, double* HR, int64_t ncells,
+                         void* stream) {
+  if (!h || !T || ncells < 0) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (ncells == 0) return 0;
+  const long long grid = std::min<long long>((ncells + 255) / 256, (long long)h->sm_count * 8);
+  thermo_hr_kernel<<<(unsigned)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(h->mech, T, IR, Hi, HR, ncells);
+  CK(cudaGetLastError());
+  h->launches++;
+  return 0;
+}
+
+int b200chem_h_given_t(b200chem_handle h, const double* T, double* Hi_mks, int64_t ncells, void* stream) {
+  if (!Hi_mks) return set_err(B200CHEM_EINVAL, "null output");
+  return thermo_launch(h, T, nullptr, Hi_mks, nullptr, ncells, stream);
+}
+
+int b200chem_heat_release(b200chem_handle h, const double* T, const double* I_R_mks, double* HR_mks, int64_t ncells,
+                          void* stream) {
+  if (!I_R_mks || !HR_mks) return set_err(B200CHEM_EINVAL, "null array");
+  return thermo_launch(h, T, I_R_mks, nullptr, HR_mks, ncells, stream);
 }
 
 }  // extern "C"

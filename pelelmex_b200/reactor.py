@@ -367,6 +367,24 @@ class ReactorB200:
                                                   T.shape[0], _stream_ptr(stream)))
         return T
 
+    def h_given_t(self, T, stream=None):
+        """getHGivenT (Source/PeleLMeX_K.H:598-615): [N, ncells] species enthalpies, J/kg."""
+        self._need()
+        Hi = _torch().empty((self.N, T.shape[0]), dtype=T.dtype, device=T.device)
+        _lib.check(_lib.load().b200chem_h_given_t(self._h, T.data_ptr(), Hi.data_ptr(), T.shape[0],
+                                                  _stream_ptr(stream)))
+        return Hi
+
+    def heat_release(self, T, I_R, stream=None):
+        """getHeatRelease (Source/PeleLMeX_Reactions.cpp:477-506): [ncells] HRR, W/m^3."""
+        self._need()
+        if I_R.shape != (self.N, T.shape[0]) or not I_R.is_contiguous():
+            raise ValueError("I_R must be a contiguous [N, ncells] tensor")
+        HR = _torch().empty_like(T)
+        _lib.check(_lib.load().b200chem_heat_release(self._h, T.data_ptr(), I_R.data_ptr(), HR.data_ptr(), T.shape[0],
+                                                     _stream_ptr(stream)))
+        return HR
+
 
 def _stream_ptr(stream):
     if stream is None:

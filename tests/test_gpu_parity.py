@@ -312,3 +312,22 @@ def test_inst_rr_and_t_from_hy(orc_cache):
     r.t_from_hy(_dev(rhoY_mks), _dev(rhoH_mks), T2)
     assert np.max(np.abs(T2.cpu().numpy() - f.T) / f.T) < 1e-10
     r.close()
+
+
+def test_h_given_t_and_heat_release():
+    """getHGivenT / getHeatRelease (Source/PeleLMeX_K.H:598-615,
+    Source/PeleLMeX_Reactions.cpp:477-506) against the NASA-7 restatement."""
+    name = "synth_ch4_21"
+    mech = M.builtin(name)
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 777, seed=12))
+    rng = np.random.default_rng(6)
+    IR = rng.normal(0.0, 1.0, (mech.n_species, f.ncells)) * f.rhoY * 1e3 * 1e4  # kg/m^3/s
+    r = ReactorB200(name).init()
+    Hi = r.h_given_t(_dev(f.T)).cpu().numpy()
+    ref = (M.h_RT(mech, f.T) * M.R_CGS * f.T[:, None] / mech.mw()).T * 1e-4  # J/kg, [N, ncells]
+    assert np.max(np.abs(Hi - ref) / np.maximum(np.abs(ref), 1e3)) < 1e-13
+    HR = r.heat_release(_dev(f.T), _dev(IR)).cpu().numpy()
+    href = -np.sum(ref * IR, axis=0)
+    scale = np.sum(np.abs(ref * IR), axis=0)
+    assert np.max(np.abs(HR - href) / scale) < 1e-13
+    r.close()
