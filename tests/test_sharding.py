@@ -64,3 +64,31 @@ def test_two_gloo_ranks_shard_and_reduce():
         assert allc == list(range(1001)) and len(set(got_c[0]) & set(got_c[1])) == 0
         assert ms == 7.0
         assert cn == {"nfe": 21, "nst": 6, "max_nfe": 14}
+
+
+def test_knapsack_balances_uneven_boxes():
+    rng = np.random.default_rng(3)
+    # an AMR-like list: a few expensive igniting boxes among many cheap ones
+    costs = np.concatenate([rng.uniform(1, 2, 30), rng.uniform(50, 80, 10)])
+    world = 4
+    rr = np.arange(costs.size) % world
+    ks = sharding.knapsack(costs, world)
+    assert sharding.efficiency(costs, ks, world) > 0.9  # 10 heavy boxes on 4 ranks: 3-3-2-2 at best
+    assert sharding.efficiency(costs, ks, world) > sharding.efficiency(costs, rr, world)
+    # every box owned once, box-count cap respected
+    capped = sharding.knapsack(costs, world, nmax=10)
+    assert np.bincount(capped, minlength=world).max() <= 10
+
+
+def test_rebalance_follows_the_threshold_rule():
+    costs = np.array([10.0, 1.0, 1.0, 1.0, 10.0, 1.0, 1.0, 1.0])
+    world = 2
+    skewed = np.array([0, 1, 1, 1, 0, 1, 1, 1])   # both heavy boxes on rank 0
+    owner, cur, test = sharding.rebalance(costs, skewed, world, threshold=1.1)
+    assert test > 1.1 * cur and not np.array_equal(owner, skewed)
+    assert sharding.efficiency(costs, owner, world) == test
+    balanced = sharding.knapsack(costs, world)
+    owner2, cur2, test2 = sharding.rebalance(costs, balanced, world, threshold=1.1)
+    assert np.array_equal(owner2, balanced)  # no gain above the threshold: keep
+    # the cost of a box is the sum of its cells' fctCount
+    assert np.allclose(sharding.box_costs([np.ones(8) * 3, np.arange(4)]), [24.0, 6.0])
