@@ -101,7 +101,7 @@ def test_random_field_sample_matches_oracle(orc_cache):
     assert (g["status"] == 0).all() and o["nfail"] == 0
     assert (np.abs(g["T"] - o["T"]) / o["T"]).max() <= T_RTOL
     # igniting cells at dt 5e-6 take hundreds of steps: an rtol 1e-8 solution
-    # is itself ~1e-6 (in Y) from the exact one, so Y is judged against a
+    # is itself ~1e-6 (in Y) from the exact one, so Y is compared with a
     # tight FP64 solve: the GPU's error within 3x the oracle's own
     rho = f.rhoY.sum(axis=0)
     tight = orc.react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-12, atol=1e-20, max_order=5)

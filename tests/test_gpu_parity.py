@@ -135,7 +135,7 @@ def test_dodecane_two_components_per_lane(orc_cache):
     terr = np.abs(g["T"] - o["T"]) / o["T"]
     assert terr.max() <= T_RTOL
     # These cells ignite inside the step (~350 RHS evaluations each): two rtol 1e-8
-    # solutions differ at the level of their own global error, so Y is judged
+    # solutions differ at the level of their own global error, so Y is compared
     # against a tight FP64 solve (rtol 1e-12): the GPU error must be of the same
     # size as the oracle's.
     tight = orc.react(f.rhoY, f.frhoY, f.T, f.rhoH, f.frhoH, f.dt, rtol=1e-12, atol=1e-20, max_order=5)

@@ -96,7 +96,7 @@ def test_hybrid_reactor_accuracy_and_gain():
     then react held-out cells: the cells the gate rejects carry exactly the
     plain BDF result; the accepted ones stay within the error the gate's
     checks hold the surrogate to (3e-4 relative T, 3e-4 mass-weighted Y; the
-    1e-4 bar of the headline is judged on the full field by the benchmark,
+    1e-4 bar of the headline is checked on the full field by the benchmark,
     which reports the plain BDF when the hybrid misses it); rhoH is exact;
     and the surrogate takes a share of the cells (what the network gains)."""
     from pelelmex_b200 import mechanism as M, workloads as W
