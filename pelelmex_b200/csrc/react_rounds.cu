@@ -615,6 +615,120 @@ __device__ __forceinline__ int reg_gj_inverse(const double* J, int ldj, const do
   return 0;
 }
 
+// The same inverse for 32 < n <= 64 in FP32: lane l holds rows l and l + 32
+// in registers.  The pivot key carries the row index (6 bits) instead of the
+// lane; the pivot row's owner writes it to shared memory and every lane
+// updates both of its rows from 16-byte reads of it.
+template <int n, typename LUT>
+__device__ __forceinline__ int reg_gj_inverse2(const double* J, int ldj, const double* dsc, double gamma, LUT* Xs,
+                                               int ldl, int* prow, int* pinv, LUT* Ar, int lda, int lane) {
+  static_assert(n > 32 && n <= 64 && sizeof(LUT) == 4, "two FP32 rows per lane");
+  const int r1 = lane + 32;
+  const bool row1 = r1 < n;
+  const double d0 = dsc[lane], d1 = row1 ? dsc[r1] : 1.0;
+  const double rd0 = 1.0 / d0, rd1 = 1.0 / d1;
+  LUT a0[n], a1[n];
+#pragma unroll
+  for (int j = 0; j < n; ++j) {
+    const double rdj = (j < 32) ? __shfl_sync(kFull, rd0, j) : __shfl_sync(kFull, rd1, j - 32);
+    const double m0 = ((lane == j) ? 1.0 : 0.0) - gamma * J[j * ldj + lane];
+    const double m1 = row1 ? ((r1 == j) ? 1.0 : 0.0) - gamma * J[j * ldj + r1] : 0.0;
+    a0[j] = (LUT)(m0 * d0 * rdj);
+    a1[j] = row1 ? (LUT)(m1 * d1 * rdj) : (LUT)0;
+  }
+  constexpr int kChunks = (n + 3) / 4;
+  constexpr int kBuf = 64;
+  unsigned used0 = 0, used1 = 0;
+  int step0 = -1, step1 = -1;
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    LUT* buf = Xs + (k & 1) * kBuf;
+    unsigned key = 0u;
+    if (!((used0 >> lane) & 1u)) key = (__float_as_uint(fabsf(a0[k])) & ~63u) | (unsigned)(63 - lane);
+    if (row1 && !((used1 >> lane) & 1u)) {
+      const unsigned k1 = (__float_as_uint(fabsf(a1[k])) & ~63u) | (unsigned)(63 - r1);
+      key = key > k1 ? key : k1;
+    }
+    const unsigned kmax = __reduce_max_sync(kFull, key);
+    if ((kmax >> 6) == 0u) return k + 1;  // no nonzero candidate: singular (warp-uniform)
+    const int p = 63 - (int)(kmax & 63u);
+    const int pl = p & 31;
+    if (p < 32) used0 |= 1u << pl;
+    else used1 |= 1u << pl;
+    if (lane == pl) {
+      if (p < 32) {
+        step0 = k;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+          float4 t;
+          t.x = a0[4 * c];
+          t.y = (4 * c + 1 < n) ? a0[4 * c + 1] : 0.f;
+          t.z = (4 * c + 2 < n) ? a0[4 * c + 2] : 0.f;
+          t.w = (4 * c + 3 < n) ? a0[4 * c + 3] : 0.f;
+          reinterpret_cast<float4*>(buf)[c] = t;
+        }
+      } else {
+        step1 = k;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+          float4 t;
+          t.x = a1[4 * c];
+          t.y = (4 * c + 1 < n) ? a1[4 * c + 1] : 0.f;
+          t.z = (4 * c + 2 < n) ? a1[4 * c + 2] : 0.f;
+          t.w = (4 * c + 3 < n) ? a1[4 * c + 3] : 0.f;
+          reinterpret_cast<float4*>(buf)[c] = t;
+        }
+      }
+    }
+    __syncwarp();
+    const LUT pv = buf[k];
+    if (!(fabsf(pv) > 0.f) || isnan(pv)) return k + 1;  // zero or NaN pivot (warp-uniform)
+    const LUT inv = 1.f / pv;
+    const LUT g0 = (p == lane) ? 1.f - inv : a0[k] * inv;
+    const LUT g1 = (p == r1) ? 1.f - inv : a1[k] * inv;
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) {
+      const float4 q = reinterpret_cast<const float4*>(buf)[c];
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = 4 * c + e;
+        if (j < n && j != k) {
+          a0[j] = fmaf(-g0, qv[e], a0[j]);
+          a1[j] = fmaf(-g1, qv[e], a1[j]);
+        }
+      }
+    }
+    a0[k] = (p == lane) ? inv : -g0;
+    a1[k] = (p == r1) ? inv : -g1;
+  }
+  __syncwarp();  // the row buffers live in Xs
+#pragma unroll
+  for (int j = 0; j < n; ++j) Xs[lane * ldl + j] = a0[j];
+  if (row1) {
+#pragma unroll
+    for (int j = 0; j < n; ++j) Xs[r1 * ldl + j] = a1[j];
+  }
+  pinv[lane] = step0;
+  prow[step0] = lane;
+  if (row1) {
+    pinv[r1] = step1;
+    prow[step1] = r1;
+  }
+  __syncwarp();
+  for (int h = 0; h < 2; ++h) {
+    const int i = lane + 32 * h;
+    if (i < n) {
+      const int pk = prow[i];
+      for (int j = 0; j < n; ++j) Ar[j * lda + i] = Xs[pk * ldl + pinv[j]];
+    } else if (i < lda) {
+      for (int j = 0; j < n; ++j) Ar[j * lda + i] = (LUT)0;  // column padding
+    }
+  }
+  __syncwarp();
+  return 0;
+}
+
 // Analytic Jacobian of one cell by one warp, lane per reaction: each lane
 // evaluates its reactions (rates and their derivatives) and adds their
 // contributions to a shared-memory Jacobian with atomics -- the mass-action
@@ -787,7 +901,7 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
 // Gauss-Jordan inverse of D (I - gamma J) D^-1 with D = diag(ewt) (FP32) or
 // of I - gamma J (FP64), written column-major into the cell record.
 template <int NS, typename LUT, int CPL>
-__global__ void __launch_bounds__(128, B200_GJ_MIN_CTAS) rk_gj(RoundsParams R) {
+__global__ void __launch_bounds__(128, CPL == 1 ? B200_GJ_MIN_CTAS : 2) rk_gj(RoundsParams R) {
   constexpr int n = NS + 1;
   extern __shared__ __align__(16) unsigned char dsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -824,6 +938,9 @@ __global__ void __launch_bounds__(128, B200_GJ_MIN_CTAS) rk_gj(RoundsParams R) {
     if constexpr (CPL == 1) {
       ier = reg_gj_inverse<(CPL == 1 ? n : 1), LUT>(J, RL.ldj, Dsc, gamma, A, SL.ldl, ipiv, ipiv2, Ar, RL.lda,
                                                     lane);
+    } else if constexpr (CPL == 2 && sizeof(LUT) == 4) {
+      ier = reg_gj_inverse2<(CPL == 2 ? n : 33), LUT>(J, RL.ldj, Dsc, gamma, A, SL.ldl, ipiv, ipiv2, Ar, RL.lda,
+                                                      lane);
     } else {
       ier = grp_gj_inverse<32, LUT>(J, RL.ldj, A, SL.ldl, ipiv, fcol, Dsc, n, gamma, lane);
       __syncwarp();
