@@ -266,6 +266,12 @@ int b200chem_autotune(b200chem_handle h, const double* rhoY, const double* extF_
                       const double* rhoH, const double* extF_rhoH, int64_t ncells, double dt_react,
                       int32_t max_trials, void* stream, b200chem_tuning* best, double* best_ms);
 
+/* Failure detection self-test (no reference counterpart): launches one
+ * thread that waits, with the bounded polling loop of the tensor-core
+ * kernels, on an mbarrier nothing arrives at; after `polls` polls (1..2^22)
+ * it sets *err (device int) to 1 and returns, leaving the context usable. */
+int b200chem_selftest_bounded_wait(int* err, int polls, void* stream);
+
 /* ---------------------------------------------------- kernel profile
  * Per-kernel CUDA-event timing of the round-based integrator (no reference
  * counterpart).  Between profile_begin and profile_end every react call

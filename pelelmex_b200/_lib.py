@@ -128,6 +128,8 @@ def load(path: os.PathLike | None = None):
     L.b200chem_advance_chemistry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChemBox), ctypes.c_int32,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_advance_chemistry.restype = ctypes.c_int
+    L.b200chem_selftest_bounded_wait.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    L.b200chem_selftest_bounded_wait.restype = ctypes.c_int
     L.b200chem_profile_begin.argtypes = [ctypes.c_void_p]
     L.b200chem_profile_end.argtypes = [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]
     for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune", "b200chem_profile_begin",

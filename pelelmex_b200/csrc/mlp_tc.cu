@@ -607,6 +607,24 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   }
 }
 
+// Self-test of the bounded waits: one thread waits on an mbarrier that
+// nothing arrives at, with the same polling loop as the GEMM roles but a
+// caller-given bound, then raises the error flag and returns -- the path a
+// GEMM takes when a copy or an MMA never completes.
+__global__ void bounded_wait_selftest(int* err, int polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    bool done = false;
+    for (int i = 0; i < polls && !done; ++i) {
+      done = mbar_try_wait(&bar, 0u);
+      if (!done && i > 64) __nanosleep(64);
+    }
+    if (!done) atomicExch(err, 1);
+  }
+}
+
 }  // namespace mlp
 }  // namespace b200
 
@@ -713,5 +731,11 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
   const int tiles = (M / kTileM) * ((N + NT - 1) / NT);
   const int grid = tiles < sms ? tiles : sms;
   gemm_bf16_tc<<<grid, kThreads, smem, st>>>(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" int b200chem_selftest_bounded_wait(int* err, int polls, void* stream) {
+  if (!err || polls < 1 || polls > (1 << 22)) return -1;
+  bounded_wait_selftest<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(err, polls);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -85,3 +85,22 @@ def test_gemm_partial_columns():
     ref = A.float() @ B.float().T
     assert torch.allclose(C[:, :22], ref[:, :22], atol=1e-2, rtol=1e-3)
     assert torch.all(C[:, 22:] == 7.0)
+
+
+def test_bounded_wait_times_out_and_context_survives():
+    """A wait on an mbarrier that nothing completes gives up after its bound
+    and raises the error flag; the next GEMM on the same context is exact."""
+    import time
+    err = torch.zeros(1, dtype=torch.int32, device=DEV)
+    t0 = time.perf_counter()
+    code = _lib.load().b200chem_selftest_bounded_wait(err.data_ptr(), 4096,
+                                                      torch.cuda.current_stream().cuda_stream)
+    assert code == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1 and time.perf_counter() - t0 < 5.0
+    M, N, K = 256, 256, 256
+    A = torch.randn((M, K), device=DEV).to(torch.bfloat16)
+    B = torch.randn((N, K), device=DEV).to(torch.bfloat16)
+    C = gemm(A, B, None)
+    ref = A.float() @ B.float().T
+    assert (C - ref).abs().max().item() <= 1e-4 * 16 * ref.abs().max().item()
