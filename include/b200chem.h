@@ -223,6 +223,13 @@ typedef struct b200chem_chem_box {
 int b200chem_advance_chemistry(b200chem_handle h, const b200chem_chem_box* boxes, int32_t nbox, double dt,
                                void* stream, int32_t* cell_status, b200chem_stats* stats);
 
+/* 64-bit FNV-1a digest of a mechanism description (its arrays in
+ * declaration order), and the species count of the generated right-hand
+ * side built into the library for that digest (0: none; react then reads
+ * the mechanism from the constant bank or global tables).  Host only. */
+uint64_t b200chem_mechanism_digest(const b200chem_mech_desc* md);
+int b200chem_generated_species(uint64_t digest);
+
 /* ReactorBase::close (Source/PeleLMeX.cpp:26). */
 int b200chem_destroy(b200chem_handle h);
 

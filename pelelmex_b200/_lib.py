@@ -128,6 +128,10 @@ def load(path: os.PathLike | None = None):
     L.b200chem_advance_chemistry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChemBox), ctypes.c_int32,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_advance_chemistry.restype = ctypes.c_int
+    L.b200chem_mechanism_digest.argtypes = [ctypes.POINTER(MechDesc)]
+    L.b200chem_mechanism_digest.restype = ctypes.c_uint64
+    L.b200chem_generated_species.argtypes = [ctypes.c_uint64]
+    L.b200chem_generated_species.restype = ctypes.c_int
     L.b200chem_selftest_bounded_wait.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     L.b200chem_selftest_bounded_wait.restype = ctypes.c_int
     L.b200chem_profile_begin.argtypes = [ctypes.c_void_p]

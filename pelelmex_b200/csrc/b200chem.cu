@@ -717,6 +717,40 @@ extern "C" {
 int b200chem_version(void) { return B200CHEM_VERSION; }
 const char* b200chem_last_error(void) { return g_err.c_str(); }
 
+// FNV-1a digest of a mechanism description over its arrays in declaration
+// order, as pelelmex_b200.mechgen.mechanism_digest computes it.
+static unsigned long long mech_digest(const b200chem_mech_desc* md) {
+  const int N = md->n_species, R = md->n_reactions;
+  unsigned long long hsh = 0xcbf29ce484222325ull;
+  auto fnv = [&](const void* p, size_t bytes) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < bytes; ++i) {
+      hsh ^= c[i];
+      hsh *= 0x100000001b3ull;
+    }
+  };
+  const int32_t hdr3[3] = {md->n_species, md->n_reactions, md->n_eff};
+  fnv(hdr3, sizeof(hdr3));
+  fnv(md->mw, sizeof(double) * N);
+  fnv(md->nasa, sizeof(double) * 15 * (size_t)N);
+  fnv(md->rtype, sizeof(int32_t) * R);
+  fnv(md->rflags, sizeof(int32_t) * R);
+  fnv(md->arr, sizeof(double) * 3 * (size_t)R);
+  fnv(md->arr_lo, sizeof(double) * 3 * (size_t)R);
+  fnv(md->arr_rev, sizeof(double) * 3 * (size_t)R);
+  fnv(md->troe, sizeof(double) * 4 * (size_t)R);
+  fnv(md->sp, sizeof(int32_t) * 8 * (size_t)R);
+  fnv(md->nu, sizeof(int32_t) * 8 * (size_t)R);
+  fnv(md->eff_ptr, sizeof(int32_t) * (R + 1));
+  fnv(md->eff_sp, sizeof(int32_t) * (size_t)md->n_eff);
+  fnv(md->eff_val, sizeof(double) * (size_t)md->n_eff);
+  return hsh;
+}
+
+uint64_t b200chem_mechanism_digest(const b200chem_mech_desc* md) { return md ? mech_digest(md) : 0; }
+
+int b200chem_generated_species(uint64_t digest) { return rounds_generated_for(digest); }
+
 b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opts* o) {
   if (!md || !o) {
     set_err(B200CHEM_EINVAL, "null mechanism or options");
@@ -809,33 +843,8 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
     }
   }
   incptr[N] = (int)incrxn.size();
-  // mechanism digest (FNV-1a over the description arrays, as pelelmex_b200.mechgen)
-  {
-    unsigned long long hsh = 0xcbf29ce484222325ull;
-    auto fnv = [&](const void* p, size_t bytes) {
-      const unsigned char* c = static_cast<const unsigned char*>(p);
-      for (size_t i = 0; i < bytes; ++i) {
-        hsh ^= c[i];
-        hsh *= 0x100000001b3ull;
-      }
-    };
-    const int32_t hdr3[3] = {md->n_species, md->n_reactions, md->n_eff};
-    fnv(hdr3, sizeof(hdr3));
-    fnv(md->mw, sizeof(double) * N);
-    fnv(md->nasa, sizeof(double) * 15 * (size_t)N);
-    fnv(md->rtype, sizeof(int32_t) * R);
-    fnv(md->rflags, sizeof(int32_t) * R);
-    fnv(md->arr, sizeof(double) * 3 * (size_t)R);
-    fnv(md->arr_lo, sizeof(double) * 3 * (size_t)R);
-    fnv(md->arr_rev, sizeof(double) * 3 * (size_t)R);
-    fnv(md->troe, sizeof(double) * 4 * (size_t)R);
-    fnv(md->sp, sizeof(int32_t) * 8 * (size_t)R);
-    fnv(md->nu, sizeof(int32_t) * 8 * (size_t)R);
-    fnv(md->eff_ptr, sizeof(int32_t) * (R + 1));
-    fnv(md->eff_sp, sizeof(int32_t) * (size_t)md->n_eff);
-    fnv(md->eff_val, sizeof(double) * (size_t)md->n_eff);
-    h->gen_mech = (rounds_generated_for(hsh) == N) ? 1 : 0;
-  }
+  // a generated right-hand side is used when the description's digest matches
+  h->gen_mech = (rounds_generated_for(mech_digest(md)) == N) ? 1 : 0;
   // packed constant-memory table of the round integrator's right-hand side
   std::vector<unsigned char> cblob;
   {

@@ -42,3 +42,23 @@ def test_null_handle_is_rejected_without_gpu():
     dt = ctypes.c_double(1e-6)
     assert L.b200chem_react(None, None, 0, ctypes.byref(dt), None, None, None, None) == -1
     assert b"bad arguments" in L.b200chem_last_error()
+
+
+def test_mechanism_digest_selects_generated_code():
+    """The library's FNV-1a digest of a mechanism description equals the
+    generator's, so the generated right-hand side of each bundled mechanism
+    is the one react uses; any change to the description selects none."""
+    import numpy as np
+    from pelelmex_b200 import _lib, mechanism as M, mechgen
+    L = _lib.load()
+    for name in ("synth_h2_9", "synth_ch4_21", "synth_c12_53"):
+        flat = M.flatten(M.builtin(name))
+        desc = flat.ctypes_desc()
+        d = L.b200chem_mechanism_digest(ctypes.byref(desc))
+        assert d == mechgen.mechanism_digest(flat)
+        assert L.b200chem_generated_species(d) == flat.n_species
+        flat.arrays["arr"][0, 0] = np.nextafter(flat.arrays["arr"][0, 0], 0.0)  # one ulp off one rate
+        desc2 = flat.ctypes_desc()
+        d2 = L.b200chem_mechanism_digest(ctypes.byref(desc2))
+        assert d2 != d and d2 == mechgen.mechanism_digest(flat)
+        assert L.b200chem_generated_species(d2) == 0
