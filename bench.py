@@ -200,6 +200,32 @@ def cpu_sample_run(mech, args, seconds: float, nthreads: int = 0):
         n = min(total, int(n * min(8.0, max(1.5, 0.6 * seconds / max(el, 1e-3)))))
 
 
+def sample_accuracy(mech, field, rY_dev, T_dev, n=2048):
+    """Max errors of the GPU result on n seeded cells: against the oracle at
+    rtol 1e-8 / atol 1e-12 and against the oracle at rtol 1e-12 / atol 1e-20;
+    the oracle's own error against the tight solve beside them."""
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    idx = workloads.sample_cells(field.ncells, min(n, field.ncells), seed=2468)
+    sub = field.subset(idx)
+    it = __import__("torch").as_tensor(idx, device=T_dev.device)
+    gT = T_dev.index_select(0, it).cpu().numpy()
+    gY = rY_dev.index_select(1, it).cpu().numpy()
+    o = orc.Oracle(mechmod.flatten(mech))
+    kw = dict(max_order=QMAX, max_steps=MAXSTEPS, nthreads=orc.max_threads())
+    ref = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=RTOL, atol=ATOL, **kw)
+    tight = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=1e-12, atol=1e-20, **kw)
+    rho = sub.rhoY.sum(axis=0)
+
+    def err(T, Y, RT, RY):
+        return {"max_rel_T": float(np.max(np.abs(T - RT) / RT)),
+                "max_abs_Y": float(np.max(np.abs(Y - RY).max(axis=0) / rho))}
+    return {"sample_cells": int(len(idx)), "gpu_vs_oracle": err(gT, gY, ref["T"], ref["rhoY"]),
+            "gpu_vs_tight": err(gT, gY, tight["T"], tight["rhoY"]),
+            "oracle_vs_tight": err(ref["T"], ref["rhoY"], tight["T"], tight["rhoY"]),
+            "tight": "oracle BDF at rtol 1e-12 / atol 1e-20", "tolerances": f"rtol {RTOL:g} / atol {ATOL:g}"}
+
+
 def emit(line):
     print(json.dumps(line), flush=True)
 
@@ -430,6 +456,12 @@ def run_b200(args, rank, world, local_rank):
     r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
     prof = r.profile_end()
     torch.cuda.nvtx.range_pop()
+    # accuracy on a seeded sample of the field: the GPU result of this call
+    # against the CPU oracle at the same tolerances and against a tight FP64
+    # solve (rtol 1e-12)
+    accuracy = None
+    if rank == 0 and not args.no_cpu:
+        accuracy = sample_accuracy(mech, field, rY, T, n=2048)
     kernels, tot_ms = {}, sum(v["ms"] for k, v in prof.items() if k != "complete")
     for k in ("start", "rhs", "ctrl", "jac", "gj", "ctrl_setup"):
         v = prof[k]
@@ -490,7 +522,7 @@ def run_b200(args, rank, world, local_rank):
               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded flame-like field; synthetic "
               "drm19-shaped mechanism)", "config": cfg, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
               "gpu_launches": launches if path != "hybrid" else hybrid["gpu_launches"], "clocks": clk.summary(),
-              "plain_gpu_bdf": plain, "hybrid": hybrid,
+              "plain_gpu_bdf": plain, "hybrid": hybrid, "accuracy": accuracy,
               "counters": {k: int(v) for k, v in counters.items()}})
     r.close()
 
