@@ -173,6 +173,31 @@ def fp64_peak_tflops(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def fp32_peak_tflops(torch, dev):
+    """Live FP32 (CUDA-core) reference peak: cuBLAS SGEMM 8192^3 without
+    TF32, best of 5."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(n, n, dtype=torch.float32, device=dev)
+        b = torch.randn(n, n, dtype=torch.float32, device=dev)
+        for _ in range(2):
+            torch.matmul(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def sample_field(mech, args, n, seed):
     """n seeded random cells of the full field, generated directly."""
     from pelelmex_b200 import workloads
@@ -499,6 +524,15 @@ def run_b200(args, rank, world, local_rank):
     fl_cell = perfmodel.flops_per_cell(counts, cn["nfe"], cn["nje"], cn["nlu"], cn["nfe"], cn["nst"])
     achieved = fl_cell * nc / (ms * 1e-3) / 1e12
     peak = fp64_peak_tflops(torch, dev)
+    # FP32 view of the inversion kernel: Gauss-Jordan inverse of the n x n
+    # Newton matrix, n^3 multiply-adds per setup
+    n1 = N + 1
+    gj_ms = kernels["gj"]["ms"]
+    gj_tf = kernels["gj"]["cells"] * 2.0 * n1 ** 3 / (gj_ms * 1e-3) / 1e12 if gj_ms else None
+    p32 = fp32_peak_tflops(torch, dev)
+    roof["fp32_view"] = {"kernel": "rk_gj (FP32 Gauss-Jordan inverse, 2 n^3 flops per setup)", "achieved": gj_tf,
+                         "peak": p32, "unit": "TFLOP/s", "frac": gj_tf / p32 if gj_tf else None,
+                         "peak_source": "measured live: cuBLAS SGEMM 8192^3 without TF32, best of 5"}
     roof["fp64_view"] = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "kernel": "one react call: rk_rhs / rk_ctrl / rk_jac / rk_gj rounds",
                          "peak_source": "measured live: cuBLAS DGEMM 8192^3 best of 5 (FP64 has no entry in the "
