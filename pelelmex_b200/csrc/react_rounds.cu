@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(128) rk_jac(RoundsParams R) {
 // Minimum resident CTAs per SM requested for the inversion kernel (bounds
 // its registers per thread).
 #ifndef B200_GJ_MIN_CTAS
-#define B200_GJ_MIN_CTAS 4
+#define B200_GJ_MIN_CTAS 6
 #endif
 
 // Newton-matrix inverse of the cells of the setup list, one warp per cell:
