@@ -72,7 +72,7 @@ def parse():
 # dram__bytes_read.sum + dram__bytes_write.sum summed over every rk_ctrl
 # launch of the kernel-profile pass of `bench.py --cells 262144`, divided by
 # the cells those launches processed.
-CTRL_DRAM_BYTES_PER_CELL = 10055.0
+CTRL_DRAM_BYTES_PER_CELL = 10050.0
 
 
 def workload_config(args):

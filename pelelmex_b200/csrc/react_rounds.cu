@@ -853,13 +853,14 @@ __device__ __forceinline__ void warp_jac(const DevMech& m, const GrpScratch& s, 
 // jbad rule marks stale: the analytic FP64 Jacobian (column-major) into the
 // cell record, one warp per cell.
 // Minimum resident CTAs per SM requested for the Jacobian kernel (bounds
-// its registers per thread).
+// its registers per thread; n > 32 keeps 2: its shared memory allows no
+// more).
 #ifndef B200_JAC_MIN_CTAS
 #define B200_JAC_MIN_CTAS 8
 #endif
 
 template <int NS, int CPL>
-__global__ void __launch_bounds__(128, B200_JAC_MIN_CTAS) rk_jac(RoundsParams R) {
+__global__ void __launch_bounds__(128, CPL == 1 ? B200_JAC_MIN_CTAS : 2) rk_jac(RoundsParams R) {
   constexpr int n = NS + 1;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ DevMech s_mech;
