@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define B200CHEM_VERSION 1
+#define B200CHEM_VERSION 2
 
 /* ---------------------------------------------------------------- errors */
 #define B200CHEM_OK 0
@@ -180,13 +180,15 @@ int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY
                         const int32_t* mask, int64_t ncells, double* dt_react, double* time,
                         void* stream, int32_t* cell_status, b200chem_stats* stats);
 
-/* Allocation-free form of b200chem_react_flat (same arguments, same results).
+/* Allocation-free form of b200chem_react_flat: same arguments, and the
+ * results of b200chem_react_flat with opts.kernel = 2 (the group integrator).
  * No reference counterpart: PelePhysics has no allocation-free react.  It
  * calls no cudaMalloc/cudaFree or other allocating routine: its scratch is a
  * fixed 24 MiB device array of the library, whose address is looked up once
  * per device (cudaGetSymbolAddress) on the first call on that device -- make
  * that first call before any stream capture.  It runs the group integrator
- * (opts.kernel 0 or 2) with the grid capped to fit the fixed scratch, and
+ * (opts.kernel 0 or 2; other values give B200CHEM_EINVAL) with the grid
+ * capped to fit the fixed scratch, and
  * returns B200CHEM_ETOOBIG when one CTA per SM of the mechanism's integrator
  * scratch does not fit.  The scratch is shared by all handles on a device:
  * calls that overlap in time (other streams, other host threads) race on it
@@ -204,7 +206,14 @@ int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* e
  * MKS (:111-120), and the reaction term I_R = -(rhoY_old - rhoY_new) / dt -
  * extF_rhoY (:153-160).  extF_rhoY / extF_rhoH are scaled in place and back,
  * as the reference does.  All boxes of the list go through one prologue
- * launch, one react and one epilogue launch. */
+ * launch, one react and one epilogue launch.
+ *
+ * skip_react != 0 is the covered-box branch of advanceChemistryBAChem
+ * (Source/PeleLMeX_Reactions.cpp:260-289, m_baChemFlag == 0): the box goes
+ * through the unit conversions and gets I_R, but is not reacted; its cells
+ * keep their state, get fctCount = 0 and status B200CHEM_CELL_MASKED, and
+ * count as masked in the statistics.  Zero (the value of a zero-initialised
+ * struct) reacts the box, as advanceChemistry does. */
 typedef struct b200chem_chem_box {
   int32_t lo[3], hi[3];
   b200chem_array4 rhoY_old;  /* N comps, in,  kg/m^3                      */
@@ -218,10 +227,33 @@ typedef struct b200chem_chem_box {
   b200chem_array4 fctCount;  /* 1 comp,  out (p may be NULL)              */
   b200chem_iarray4 mask;     /* 1 comp,  in, 0 = skip (p may be NULL)     */
   b200chem_array4 I_R;       /* N comps, out, kg/m^3/s (p may be NULL)    */
+  int32_t skip_react;        /* != 0: covered box, not reacted (BAChem)   */
+  int32_t reserved;
 } b200chem_chem_box;
 
 int b200chem_advance_chemistry(b200chem_handle h, const b200chem_chem_box* boxes, int32_t nbox, double dt,
                                void* stream, int32_t* cell_status, b200chem_stats* stats);
+
+/* ------------------------------------------------ chemistry forcing
+ * PeleLM::getScalarReactForce (Source/PeleLMeX_Reactions.cpp:437-475), MKS:
+ * the external forcing of the next react from the advection-diffusion
+ * update of this step,
+ *   extF_rhoY_k = (rhoY_new_k - rhoY_old_k) * (1/dt) - I_R_k
+ *   extF_rhoH   = (rhoH_new - rhoH_old) * (1/dt)
+ * with 1/dt rounded once on the host and every product and difference
+ * rounded separately, as the reference writes it.  All boxes in one launch. */
+typedef struct b200chem_force_box {
+  int32_t lo[3], hi[3];
+  b200chem_array4 rhoY_old;  /* N comps, in,  kg/m^3    (state at t^n)            */
+  b200chem_array4 rhoH_old;  /* 1 comp,  in,  J/m^3                               */
+  b200chem_array4 rhoY_new;  /* N comps, in,  kg/m^3    (advection-diffusion state) */
+  b200chem_array4 rhoH_new;  /* 1 comp,  in,  J/m^3                               */
+  b200chem_array4 I_R;       /* N comps, in,  kg/m^3/s  (last reaction term)       */
+  b200chem_array4 extF_rhoY; /* N comps, out, kg/m^3/s                            */
+  b200chem_array4 extF_rhoH; /* 1 comp,  out, J/m^3/s                             */
+} b200chem_force_box;
+
+int b200chem_react_force(b200chem_handle h, const b200chem_force_box* boxes, int32_t nbox, double dt, void* stream);
 
 /* 64-bit FNV-1a digest of a mechanism description (its arrays in
  * declaration order), and the species count of the generated right-hand
@@ -353,46 +385,100 @@ int b200chem_heat_release(b200chem_handle h, const double* T, const double* I_R_
  * K % 16 == 0.  epi: 0 C fp32; 1 C bf16; 2 C bf16 = gelu(.), aux fp32 =
  * pre-activation (aux may be NULL); 3 C bf16 = (A.B^T) * gelu'(aux).  Only
  * columns < n_valid (0 = N) of C are written.  *err (device int, optional)
- * is set to 1 if a tensor-core completion wait timed out. */
+ * is set to 1 if a tensor-core completion wait timed out.
+ *
+ * Two-term BF16 operands (flags OR-ed into epi): a value v is carried as
+ * hi = bf16(v) and lo = bf16(v - hi), about 16 significant bits, and the
+ * products are accumulated in FP32.  B200CHEM_GEMM_SPLIT_A: A has 2K columns,
+ * [hi | lo], both multiplied by the same B (lda >= 2K; needs K <= 256, N <= 256
+ * and K <= 64 or K % 64 == 0).  B200CHEM_GEMM_SPLIT_OUT (epi 1 or 2, N <= 256):
+ * C is written as [hi | lo] (columns c and c + N; ldc >= 2N), and the
+ * pre-activations of epi 2 go to aux with row stride N. */
+#define B200CHEM_GEMM_SPLIT_OUT 0x10
+#define B200CHEM_GEMM_SPLIT_A 0x20
 int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* B, long long ldb, int M, int N, int K,
                            void* C, long long ldc, const float* bias, float* aux, int epi, int n_valid, int* err,
                            void* stream);
 
-/* Acceptance thresholds of a surrogate prediction (b200chem_surrogate_gate). */
-typedef struct b200chem_gate_opts {
-  double rtol;      /* relative tolerance of the one-step implicit residual        */
-  double atol;      /* absolute tolerance, times rho (species) or T (temperature) */
-  double tol_T;     /* |T(h, Y_pred) - (T0 + dT_pred)| bound, K                     */
-  double tol_elem;  /* element-conservation bound, relative to the atom content   */
-  double tol_mass;  /* |sum Y_pred - 1| bound (and most negative Y tolerated)     */
-  double rchange;   /* residual tolerance relative to the step change |y1 - y0|   */
-  double dT_max;    /* > 0: predictions with |dT| above it are rejected, K         */
-  int32_t t_source; /* accepted T: 0 from (h, Y) (energy exact), 1 predicted      */
-  int32_t residual_t_only; /* 1: the residual test covers the temperature only   */
-} b200chem_gate_opts;
+/* Fused Adam step (Kingma & Ba 2015) of one FP32 parameter tensor [rows][cols]
+ * of the network, step = 1, 2, ... (bias corrections), in place on p, m, v
+ * with gradient g; then writes the BF16 copies the GEMMs read: wb [rows][cols]
+ * and wbt [cols][rows] (each may be NULL).  All device pointers. */
+int b200chem_mlp_adam(float* p, const float* g, float* m, float* v, int rows, int cols, float lr, float beta1,
+                      float beta2, float eps, int step, void* wb, void* wbt, void* stream);
 
-/* Network input of the surrogate for ncells cells (component-major CGS rhoY
- * [N][ncells], T [ncells]): x_bf16 [nrows][in] with in = N + 2 rounded up to a
- * multiple of 16, rows ncells..nrows-1 zero; nrows % 128 == 0.  Columns:
- * (T, log10(Y_k + 1e-20), log10 dt), each standardised by xmean/xstd [N + 2]. */
-int b200chem_surrogate_features(b200chem_handle h, const double* rhoY, const double* T, int64_t ncells,
-                                int64_t nrows, double dt, const float* xmean, const float* xstd, void* x_bf16,
-                                void* stream);
+/* ----------------------------------------------------- hybrid reactor
+ * No reference counterpart: the surrogate-first react.  An ensemble of
+ * networks predicts every cell's change over dt_react; a prediction is
+ * accepted only when the acceptance rule below holds, and the accepted state
+ * is corrected to conserve the element totals and the energy exactly; the
+ * other cells are integrated by the BDF of b200chem_react_flat.
+ *
+ * Weights file (b200chem_surrogate_load), little endian:
+ *   header (header_bytes, >= 128):
+ *     0  char[8]  "B2CHSURR"           8  u32 version (1)   12 u32 header_bytes
+ *     16 u64 mechanism digest (b200chem_mechanism_digest of the description
+ *        the networks were trained for; loading for another mechanism fails)
+ *     24 i32[12] N, N + 2, N + 1, hidden (256), in (N + 2 padded to 16),
+ *        out (N + 1 padded to 16), members (1..16), terms (1 or 2), dtype (1:
+ *        BF16 weights, FP32 biases), min_members, n_elements (0..8), 0
+ *     72 f64[7] the acceptance rule it was calibrated for: t_rel, spread,
+ *        dT_cap, gap, tol_elem, tol_mass, resid
+ *   body: xmean, xstd [N + 2] f32; ymean, ystd [N + 1] f32; s [N + 1] f64
+ *   (asinh scales); elem [n_elements][N] f64 (atoms per species); then per
+ *   member W0 [256][in] bf16, b0 [256] f32, W1, b1, W2, b2 ([256][256] bf16,
+ *   [256] f32), W3 [out][256] bf16, b3 [out] f32.
+ * A member maps x = (T, log10(Y_k + 1e-20), log10 dt), standardised, through
+ * three GELU layers to u; the change is dy_j = s_j sinh(u_j ystd_j + ymean_j)
+ * (dT, then dY_k). */
+typedef struct b200chem_hybrid_opts {
+  double t_rel;    /* relative T error allowed to an accepted cell: a "bar" is t_rel * T1 */
+  double spread;   /* max |dT_member - dT_mean|, in bars                                 */
+  double dT_cap;   /* max |dT_mean|, in bars                                              */
+  double gap;      /* max |T(h1, Y_pred) - T1| before the energy projection, in bars      */
+  double tol_elem; /* raw element-conservation error, relative to the atom content       */
+  double tol_mass; /* raw mass-conservation error, relative; also the most negative
+                      partial density tolerated (then clipped)                            */
+  double resid;    /* > 0: |T1 - T0 - dt/2 (f_T(y0) + f_T(y1))| bound in bars (two RHS)  */
+  int32_t min_members; /* fewer members in the surrogate than this: EINVAL                */
+  int32_t reserved;
+} b200chem_hybrid_opts;
 
-/* Acceptance gate of a surrogate prediction (pred [ncells][out] FP32,
- * out = N + 1 rounded up to a multiple of 16, standardised; ymean/ystd
- * [N + 1]): mass and element conservation of the raw prediction (then an
- * exact element-conserving correction), T from (h, Y) against the predicted
- * dT, and (rtol > 0) a one-step implicit residual with two right-hand sides.
- * Accepted cells are advanced in place (rhoY, T, rhoH, fctCount) and get
- * accept[c] = 1; the others are left untouched with accept[c] = -(first
- * failed check): -1 mass, -2 elements, -3 energy, -4 residual, -5 change
- * cap.  elem
- * [n_elements][N] holds the atoms of each element in each species. */
-int b200chem_surrogate_gate(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T, double* rhoH,
-                            const double* extF_rhoH, double* fctCount, int64_t ncells, double dt, const float* pred,
-                            const float* ymean, const float* ystd, const double* elem, int32_t n_elements,
-                            const b200chem_gate_opts* opts, int32_t* accept, void* stream);
+typedef struct b200chem_hybrid_stats {
+  int64_t predicted, accepted;
+  int64_t rejected_spread, rejected_cap, rejected_mass, rejected_elements, rejected_energy, rejected_negative,
+      rejected_residual, rejected_nonfinite;
+} b200chem_hybrid_stats;
+
+typedef struct b200chem_surrogate* b200chem_surrogate_handle;
+
+/* Loads an ensemble (the weights file above, from memory or from a path) to
+ * the reactor's device, which must be current.  NULL on failure (message in
+ * b200chem_last_error). */
+b200chem_surrogate_handle b200chem_surrogate_load(b200chem_handle h, const void* data, size_t nbytes);
+b200chem_surrogate_handle b200chem_surrogate_load_file(b200chem_handle h, const char* path);
+/* The acceptance rule stored in the file. */
+int b200chem_surrogate_get_opts(b200chem_surrogate_handle s, b200chem_hybrid_opts* o);
+int b200chem_surrogate_destroy(b200chem_surrogate_handle s);
+
+/* Ensemble prediction for ncells cells (component-major CGS rhoY [N][ncells],
+ * T [ncells]): dy_mean [ncells][N + 1] (dT, dY_k; FP64) and, optionally,
+ * dT_spread [ncells], the largest deviation of a member's dT from the mean.
+ * Synchronous. */
+int b200chem_surrogate_infer(b200chem_surrogate_handle s, const double* rhoY, const double* T, int64_t ncells,
+                             double dt, double* dy_mean, double* dT_spread, void* stream);
+
+/* Surrogate-first form of b200chem_react_flat (same arrays and in-place
+ * semantics; mask == 0 cells untouched with fctCount 0).  opts NULL uses the
+ * rule stored in the weights file.  Accepted cells get fctCount = 0 (2 with
+ * the residual check) and status OK; the others carry the BDF's results.
+ * Reads the rejected count back to the host once per call.  stats and hstats
+ * (host, optional): BDF counters of the rejected cells (n_cells counts every
+ * integrated cell) and the gate's counts. */
+int b200chem_react_hybrid(b200chem_handle h, b200chem_surrogate_handle s, const b200chem_hybrid_opts* opts,
+                          double* rhoY, const double* extF_rhoY, double* T, double* rhoH, const double* extF_rhoH,
+                          double* fctCount, const int32_t* mask, int64_t ncells, double* dt_react, double* time,
+                          void* stream, int32_t* cell_status, b200chem_stats* stats, b200chem_hybrid_stats* hstats);
 
 #ifdef __cplusplus
 }

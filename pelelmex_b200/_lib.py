@@ -38,7 +38,13 @@ class ChemBox(ctypes.Structure):
     _fields_ = [("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3), ("rhoY_old", Array4), ("rhoH_old", Array4),
                 ("T_old", Array4), ("rhoY_new", Array4), ("rhoH_new", Array4), ("T_new", Array4),
                 ("extF_rhoY", Array4), ("extF_rhoH", Array4), ("fctCount", Array4), ("mask", Array4),
-                ("I_R", Array4)]
+                ("I_R", Array4), ("skip_react", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class ForceBox(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_int32 * 3), ("hi", ctypes.c_int32 * 3), ("rhoY_old", Array4), ("rhoH_old", Array4),
+                ("rhoY_new", Array4), ("rhoH_new", Array4), ("I_R", Array4), ("extF_rhoY", Array4),
+                ("extF_rhoH", Array4)]
 
 
 class Stats(ctypes.Structure):
@@ -51,10 +57,19 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-class GateOpts(ctypes.Structure):
-    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("tol_T", ctypes.c_double),
-                ("tol_elem", ctypes.c_double), ("tol_mass", ctypes.c_double), ("rchange", ctypes.c_double),
-                ("dT_max", ctypes.c_double), ("t_source", ctypes.c_int32), ("residual_t_only", ctypes.c_int32)]
+class HybridOpts(ctypes.Structure):
+    _fields_ = [("t_rel", ctypes.c_double), ("spread", ctypes.c_double), ("dT_cap", ctypes.c_double),
+                ("gap", ctypes.c_double), ("tol_elem", ctypes.c_double), ("tol_mass", ctypes.c_double),
+                ("resid", ctypes.c_double), ("min_members", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class HybridStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "predicted", "accepted", "rejected_spread", "rejected_cap", "rejected_mass", "rejected_elements",
+        "rejected_energy", "rejected_negative", "rejected_residual", "rejected_nonfinite")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Tuning(ctypes.Structure):
@@ -109,15 +124,31 @@ def load(path: os.PathLike | None = None):
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_mlp_gemm_bf16.restype = ctypes.c_int
+    L.b200chem_mlp_adam.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.b200chem_mlp_adam.restype = ctypes.c_int
     L.b200chem_surrogate_features.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, ctypes.c_int64,
-                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                              ctypes.c_void_p]
+                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                              ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_surrogate_features.restype = ctypes.c_int
-    L.b200chem_surrogate_gate.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
-                                          ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
-                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
-                                          ctypes.POINTER(GateOpts), ctypes.c_void_p, ctypes.c_void_p]
-    L.b200chem_surrogate_gate.restype = ctypes.c_int
+    L.b200chem_surrogate_load.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
+    L.b200chem_surrogate_load.restype = ctypes.c_void_p
+    L.b200chem_surrogate_load_file.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.b200chem_surrogate_load_file.restype = ctypes.c_void_p
+    L.b200chem_surrogate_get_opts.argtypes = [ctypes.c_void_p, ctypes.POINTER(HybridOpts)]
+    L.b200chem_surrogate_get_opts.restype = ctypes.c_int
+    L.b200chem_surrogate_destroy.argtypes = [ctypes.c_void_p]
+    L.b200chem_surrogate_destroy.restype = ctypes.c_int
+    L.b200chem_surrogate_infer.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int64, ctypes.c_double, _f64p,
+                                           _f64p, ctypes.c_void_p]
+    L.b200chem_surrogate_infer.restype = ctypes.c_int
+    L.b200chem_react_hybrid.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(HybridOpts), _f64p, _f64p,
+                                        _f64p, _f64p, _f64p, _f64p, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(Stats),
+                                        ctypes.POINTER(HybridStats)]
+    L.b200chem_react_hybrid.restype = ctypes.c_int
     L.b200chem_kernel_launches.argtypes = [ctypes.c_void_p]
     L.b200chem_kernel_launches.restype = ctypes.c_int64
     L.b200chem_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
@@ -128,6 +159,9 @@ def load(path: os.PathLike | None = None):
     L.b200chem_advance_chemistry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChemBox), ctypes.c_int32,
                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.b200chem_advance_chemistry.restype = ctypes.c_int
+    L.b200chem_react_force.argtypes = [ctypes.c_void_p, ctypes.POINTER(ForceBox), ctypes.c_int32, ctypes.c_double,
+                                       ctypes.c_void_p]
+    L.b200chem_react_force.restype = ctypes.c_int
     L.b200chem_mechanism_digest.argtypes = [ctypes.POINTER(MechDesc)]
     L.b200chem_mechanism_digest.restype = ctypes.c_uint64
     L.b200chem_generated_species.argtypes = [ctypes.c_uint64]

@@ -10,6 +10,10 @@
 //            :153-160)  extF_rhoH *= 0.1                       (CGS -> MKS)
 //                       I_R = -(rhoY_old - rhoY_new) / dt - extF_rhoY
 //
+// and, before the next react, the forcing of getScalarReactForce
+// (:437-475)      extF_rhoY = (rhoY_new - rhoY_old) * (1/dt) - I_R,
+//                 extF_rhoH = (rhoH_new - rhoH_old) * (1/dt).
+//
 // The arithmetic is the reference's, operation for operation, so the MKS
 // fields round the same way.  One thread per cell, grid-stride over the
 // cells of all boxes; memory-bound elementwise work.
@@ -19,7 +23,8 @@ namespace b200 {
 
 namespace {
 
-__device__ __forceinline__ void chem_locate(const ChemBoxDev* boxes, int nbox, long long cell, int* b, int* i, int* j,
+template <class Box>
+__device__ __forceinline__ void chem_locate(const Box* boxes, int nbox, long long cell, int* b, int* i, int* j,
                                             int* k) {
   int lo = 0, hi = nbox - 1;
   while (lo < hi) {
@@ -27,7 +32,7 @@ __device__ __forceinline__ void chem_locate(const ChemBoxDev* boxes, int nbox, l
     if (boxes[mid].off <= cell) lo = mid;
     else hi = mid - 1;
   }
-  const ChemBoxDev& bx = boxes[lo];
+  const Box& bx = boxes[lo];
   const long long loc = cell - bx.off;
   *b = lo;
   *i = bx.lo0 + (int)(loc % bx.nx);
@@ -72,7 +77,34 @@ __global__ void chem_epilogue(const ChemBoxDev* __restrict__ boxes, int nbox, lo
   }
 }
 
+__global__ void react_force(const ForceBoxDev* __restrict__ boxes, int nbox, long long total, int N, double dt_inv) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    int b, i, j, k;
+    chem_locate(boxes, nbox, c, &b, &i, &j, &k);
+    const ForceBoxDev& bx = boxes[b];
+    const double* yo = elem(bx.rY_o, i, j, k);
+    const double* yn = elem(bx.rY_n, i, j, k);
+    const double* ir = elem(bx.IR, i, j, k);
+    double* fy = elem(bx.fY, i, j, k);
+    // separately rounded difference, product and difference (no FMA)
+    for (int n = 0; n < N; ++n)
+      fy[n * bx.fY.ns] =
+          __dsub_rn(__dmul_rn(__dsub_rn(yn[n * bx.rY_n.ns], yo[n * bx.rY_o.ns]), dt_inv), ir[n * bx.IR.ns]);
+    *elem(bx.fH, i, j, k) = __dmul_rn(__dsub_rn(*elem(bx.rH_n, i, j, k), *elem(bx.rH_o, i, j, k)), dt_inv);
+  }
+}
+
 }  // namespace
+
+cudaError_t react_force_launch(const ForceBoxDev* d_boxes, int nbox, long long total, int N, double dt_inv,
+                               int sm_count, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  const long long need = (total + 255) / 256;
+  const int grid = (int)(need < 8LL * sm_count ? need : 8LL * sm_count);
+  react_force<<<grid, 256, 0, st>>>(d_boxes, nbox, total, N, dt_inv);
+  return cudaGetLastError();
+}
 
 cudaError_t advance_chem_launch(int phase, const ChemBoxDev* d_boxes, int nbox, long long total, int N,
                                 double dt_inv, int sm_count, cudaStream_t st) {

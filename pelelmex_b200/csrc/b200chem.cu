@@ -205,6 +205,18 @@ __global__ void thermo_hr_kernel(DevMech m, const double* __restrict__ T, const 
 }  // namespace
 
 // ------------------------------------------------------------------ handle
+// A small host-built array (box descriptors) copied to the device on the
+// caller's stream: pinned staging plus a device copy, both reused across
+// calls; the staging buffer is rewritten only after the previous call's copy
+// from it has completed.
+struct StagedBuf {
+  void* d = nullptr;
+  void* h = nullptr;
+  size_t bytes = 0;
+  bool pending = false;
+  cudaEvent_t ev = nullptr;
+};
+
 struct b200chem_reactor {
   int device = 0;
   int N = 0, R = 0, n = 0;
@@ -236,15 +248,15 @@ struct b200chem_reactor {
   unsigned char* h_cmech = nullptr;  // pinned packed constant-memory table (null: too large)
   int cmech_bytes = 0;
   int gen_mech = 0;  // 1: a generated right-hand side matches the mechanism
+  unsigned long long digest = 0;  // FNV-1a digest of the mechanism description
   b200chem_tuning tune{};           // launch shape of the round-based integrator
   cudaStream_t cap_stream = nullptr;  // private stream the round graph is captured on
   cudaGraphExec_t rgraph = nullptr;   // executable graph of rounds_per_check rounds
   int rgraph_rounds = 0;              // rounds in rgraph
-  void* d_cboxes = nullptr;           // advanceChemistry box descriptors (device, pinned staging)
-  void* h_cboxes = nullptr;
-  size_t cboxes_bytes = 0;
-  bool cboxes_pending = false;
-  cudaEvent_t cbox_ev = nullptr;
+  StagedBuf cboxes;                   // advanceChemistry box descriptors
+  StagedBuf fboxes;                   // getScalarReactForce box descriptors
+  int* d_zero_mask = nullptr;         // all-zero mask row of the covered (skip_react) boxes
+  long long zero_mask_len = 0;
   // per-kernel profile of the round integrator (b200chem_profile_begin/end)
   struct ProfRec {
     int kind;
@@ -269,6 +281,8 @@ const double* handle_atol(b200chem_handle h) { return h->d_atol; }
 int handle_device(b200chem_handle h) { return h->device; }
 void handle_count_launch(b200chem_handle h) { h->launches++; }
 int handle_set_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+unsigned long long handle_digest(b200chem_handle h) { return h->digest; }
+int handle_sm_count(b200chem_handle h) { return h->sm_count; }
 }  // namespace b200
 
 namespace {
@@ -690,6 +704,37 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   return 0;
 }
 
+// Copies `bytes` of host data to the device buffer of `b` on stream `st`
+// (through the pinned staging buffer) and returns the device pointer.
+int stage_to_device(StagedBuf& b, const void* src, size_t bytes, cudaStream_t st, void** out) {
+  if (!b.ev) CK(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming));
+  if (b.pending) CK(cudaEventSynchronize(b.ev));
+  b.pending = false;
+  if (bytes > b.bytes) {
+    if (b.d) cudaFree(b.d);
+    if (b.h) cudaFreeHost(b.h);
+    b.d = b.h = nullptr;
+    b.bytes = 0;
+    CK(cudaMalloc(&b.d, bytes));
+    CK(cudaMallocHost(&b.h, bytes));
+    b.bytes = bytes;
+  }
+  memcpy(b.h, src, bytes);
+  CK(cudaMemcpyAsync(b.d, b.h, bytes, cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(b.ev, st));
+  b.pending = true;
+  *out = b.d;
+  return 0;
+}
+
+void staged_free(StagedBuf& b) {
+  if (b.pending) cudaEventSynchronize(b.ev);
+  if (b.ev) cudaEventDestroy(b.ev);
+  if (b.d) cudaFree(b.d);
+  if (b.h) cudaFreeHost(b.h);
+  b = StagedBuf{};
+}
+
 DevArr to_dev(const b200chem_array4& a) {
   DevArr d;
   d.p = a.p;
@@ -844,7 +889,8 @@ b200chem_handle b200chem_create(const b200chem_mech_desc* md, const b200chem_opt
   }
   incptr[N] = (int)incrxn.size();
   // a generated right-hand side is used when the description's digest matches
-  h->gen_mech = (rounds_generated_for(mech_digest(md)) == N) ? 1 : 0;
+  h->digest = mech_digest(md);
+  h->gen_mech = (rounds_generated_for(h->digest) == N) ? 1 : 0;
   // packed constant-memory table of the round integrator's right-hand side
   std::vector<unsigned char> cblob;
   {
@@ -1063,35 +1109,84 @@ int b200chem_advance_chemistry(b200chem_handle h, const b200chem_chem_box* cboxe
     v.mask = x.mask;
   }
   if (total == 0) return 0;
-  // box descriptors: pinned staging, device copy (reused across calls)
-  const size_t bytes = sizeof(ChemBoxDev) * (size_t)nbox;
-  if (!h->cbox_ev) CK(cudaEventCreateWithFlags(&h->cbox_ev, cudaEventDisableTiming));
-  // the pinned staging buffer is reused once the previous call's copy from it is done
-  if (h->cboxes_pending) CK(cudaEventSynchronize(h->cbox_ev));
-  h->cboxes_pending = false;
-  if (bytes > h->cboxes_bytes) {
-    if (h->d_cboxes) cudaFree(h->d_cboxes);
-    if (h->h_cboxes) cudaFreeHost(h->h_cboxes);
-    h->d_cboxes = nullptr;
-    h->h_cboxes = nullptr;
-    h->cboxes_bytes = 0;
-    CK(cudaMalloc(&h->d_cboxes, bytes));
-    CK(cudaMallocHost(&h->h_cboxes, bytes));
-    h->cboxes_bytes = bytes;
+  // covered boxes (advanceChemistryBAChem's m_baChemFlag == 0) react through
+  // an all-zero mask: every cell is skipped, keeps its state and gets
+  // fctCount = 0 (Source/PeleLMeX_Reactions.cpp:260-289)
+  long long zlen = 0;
+  for (int b = 0; b < nbox; ++b)
+    if (cboxes[b].skip_react) zlen = std::max<long long>(zlen, cboxes[b].hi[0] - cboxes[b].lo[0] + 1);
+  if (zlen > h->zero_mask_len) {
+    if (h->d_zero_mask) {
+      CK(cudaStreamSynchronize(st));
+      cudaFree(h->d_zero_mask);
+      h->d_zero_mask = nullptr;
+      h->zero_mask_len = 0;
+    }
+    CK(cudaMalloc(&h->d_zero_mask, sizeof(int) * (size_t)zlen));
+    CK(cudaMemsetAsync(h->d_zero_mask, 0, sizeof(int) * (size_t)zlen, st));
+    h->zero_mask_len = zlen;
   }
-  memcpy(h->h_cboxes, cb.data(), bytes);
-  CK(cudaMemcpyAsync(h->d_cboxes, h->h_cboxes, bytes, cudaMemcpyHostToDevice, st));
-  CK(cudaEventRecord(h->cbox_ev, st));
-  h->cboxes_pending = true;
-  CK(advance_chem_launch(0, static_cast<const ChemBoxDev*>(h->d_cboxes), nbox, total, h->N, 0.0, h->sm_count, st));
+  for (int b = 0; b < nbox; ++b) {
+    if (!cboxes[b].skip_react) continue;
+    b200chem_iarray4& m = views[b].mask;
+    m.p = h->d_zero_mask;  // element (i, j, k) -> i - lo[0]: strides 0 across j and k
+    m.jstride = m.kstride = m.nstride = 0;
+    for (int d = 0; d < 3; ++d) {
+      m.lo[d] = cboxes[b].lo[d];
+      m.hi[d] = cboxes[b].hi[d];
+    }
+  }
+  void* d_cb = nullptr;
+  int err = stage_to_device(h->cboxes, cb.data(), sizeof(ChemBoxDev) * (size_t)nbox, st, &d_cb);
+  if (err) return err;
+  CK(advance_chem_launch(0, static_cast<const ChemBoxDev*>(d_cb), nbox, total, h->N, 0.0, h->sm_count, st));
   h->launches++;
   double dt_react = dt, time = 0.0;
-  int err = b200chem_react(h, views.data(), nbox, &dt_react, &time, stream, cell_status, stats);
+  err = b200chem_react(h, views.data(), nbox, &dt_react, &time, stream, cell_status, stats);
   if (err && err != B200CHEM_EINTEGRATE) return err;
-  CK(advance_chem_launch(1, static_cast<const ChemBoxDev*>(h->d_cboxes), nbox, total, h->N, 1.0 / dt, h->sm_count,
-                         st));
+  CK(advance_chem_launch(1, static_cast<const ChemBoxDev*>(d_cb), nbox, total, h->N, 1.0 / dt, h->sm_count, st));
   h->launches++;
   return err;
+}
+
+int b200chem_react_force(b200chem_handle h, const b200chem_force_box* fboxes, int32_t nbox, double dt,
+                         void* stream) {
+  if (!h || (!fboxes && nbox > 0) || nbox < 0) return set_err(B200CHEM_EINVAL, "bad arguments");
+  if (!(dt > 0.0)) return set_err(B200CHEM_EINVAL, "dt must be positive");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::vector<ForceBoxDev> fb(nbox);
+  long long total = 0;
+  for (int b = 0; b < nbox; ++b) {
+    const b200chem_force_box& x = fboxes[b];
+    if (!x.rhoY_old.p || !x.rhoH_old.p || !x.rhoY_new.p || !x.rhoH_new.p || !x.I_R.p || !x.extF_rhoY.p ||
+        !x.extF_rhoH.p)
+      return set_err(B200CHEM_EINVAL, "box %d: null array", b);
+    ForceBoxDev& d = fb[b];
+    d.lo0 = x.lo[0];
+    d.lo1 = x.lo[1];
+    d.lo2 = x.lo[2];
+    d.nx = x.hi[0] - x.lo[0] + 1;
+    d.ny = x.hi[1] - x.lo[1] + 1;
+    d.nz = x.hi[2] - x.lo[2] + 1;
+    if (d.nx < 1 || d.ny < 1 || d.nz < 1) return set_err(B200CHEM_EINVAL, "box %d is empty or inverted", b);
+    d.off = total;
+    total += (long long)d.nx * d.ny * d.nz;
+    d.rY_o = to_dev(x.rhoY_old);
+    d.rH_o = to_dev(x.rhoH_old);
+    d.rY_n = to_dev(x.rhoY_new);
+    d.rH_n = to_dev(x.rhoH_new);
+    d.IR = to_dev(x.I_R);
+    d.fY = to_dev(x.extF_rhoY);
+    d.fH = to_dev(x.extF_rhoH);
+  }
+  if (total == 0) return 0;
+  void* d_fb = nullptr;
+  int err = stage_to_device(h->fboxes, fb.data(), sizeof(ForceBoxDev) * (size_t)nbox, st, &d_fb);
+  if (err) return err;
+  // 1/dt once on the host, as the reference's dtinv = 1.0 / m_dt
+  CK(react_force_launch(static_cast<const ForceBoxDev*>(d_fb), nbox, total, h->N, 1.0 / dt, h->sm_count, st));
+  h->launches++;
+  return 0;
 }
 
 int b200chem_react_flat(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T, double* rhoH,
@@ -1163,6 +1258,11 @@ int noalloc_scratch(int device, unsigned char** out) {
   return 0;
 }
 
+// Stores the flat call's box descriptor into the fixed scratch.  The
+// descriptor travels as a kernel argument, so no host buffer has to outlive
+// the call.
+__global__ void noalloc_store_box(DevBox d, DevBox* dst) { *dst = d; }
+
 }  // namespace
 
 extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T,
@@ -1174,7 +1274,7 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
     return set_err(B200CHEM_EINVAL, "null state array");
   if (!(*dt_react > 0.0)) return set_err(B200CHEM_EINVAL, "dt_react must be positive");
   if (ncells > 0x7fffffffLL) return set_err(B200CHEM_ETOOBIG, "ncells above 2^31-1 in one flat call");
-  if (h->opts.kernel == 1)
+  if (h->opts.kernel != 0 && h->opts.kernel != 2)
     return set_err(B200CHEM_EINVAL, "the allocation-free react runs the group integrator only (kernel 0 or 2)");
   int dev = -1;
   CK(cudaGetDevice(&dev));
@@ -1235,8 +1335,9 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
     d.fc = mk(fctCount);
     d.mask.p = mask;
     d.mask.js = d.mask.ks = ncells;
-    // pageable source: the copy is staged before cudaMemcpyAsync returns
-    CK(cudaMemcpyAsync(d_box, &d, sizeof(DevBox), cudaMemcpyHostToDevice, st));
+    noalloc_store_box<<<1, 1, 0, st>>>(d, d_box);
+    CK(cudaGetLastError());
+    h->launches++;
     ReactParams P;
     P.mech = h->mech;
     P.boxes = d_box;
@@ -1252,6 +1353,7 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
     P.status = cell_status;
     Q.gscratch = base + kNoAllocWorkOffset;
     CK(v->launch(P, Q, (int)grid, smem, st));
+    h->launches++;
   }
   if (stats) {
     long long st_h[kStCount];
@@ -1475,10 +1577,9 @@ int b200chem_destroy(b200chem_handle h) {
   if (h->h_rcnt) cudaFreeHost(h->h_rcnt);
   if (h->h_cmech) cudaFreeHost(h->h_cmech);
   if (h->rgraph) cudaGraphExecDestroy(h->rgraph);
-  if (h->cboxes_pending) cudaEventSynchronize(h->cbox_ev);
-  if (h->cbox_ev) cudaEventDestroy(h->cbox_ev);
-  if (h->d_cboxes) cudaFree(h->d_cboxes);
-  if (h->h_cboxes) cudaFreeHost(h->h_cboxes);
+  staged_free(h->cboxes);
+  staged_free(h->fboxes);
+  if (h->d_zero_mask) cudaFree(h->d_zero_mask);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->h_pcnt) cudaFreeHost(h->h_pcnt);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);

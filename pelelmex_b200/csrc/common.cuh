@@ -38,6 +38,15 @@ struct ChemBoxDev {
 cudaError_t advance_chem_launch(int phase, const ChemBoxDev* d_boxes, int nbox, long long total, int N,
                                 double dt_inv, int sm_count, cudaStream_t st);
 
+// One box of getScalarReactForce (advance_chem.cu), MKS.
+struct ForceBoxDev {
+  int lo0, lo1, lo2, nx, ny, nz;
+  long long off;
+  DevArr rY_o, rH_o, rY_n, rH_n, IR, fY, fH;
+};
+cudaError_t react_force_launch(const ForceBoxDev* d_boxes, int nbox, long long total, int N, double dt_inv,
+                               int sm_count, cudaStream_t st);
+
 // stats slots in the scratch buffer (after the queue counter)
 enum { kStCells = 0, kStMasked, kStFailed, kStNst, kStNfe, kStNje, kStNlu, kStNetf, kStNcfn, kStMaxNfe,
        kStMaxNst, kStCount };
@@ -163,6 +172,8 @@ const double* handle_atol(b200chem_handle h);
 int handle_device(b200chem_handle h);
 void handle_count_launch(b200chem_handle h);
 int handle_set_error(int code, const char* msg);
+unsigned long long handle_digest(b200chem_handle h);  // FNV-1a digest of the mechanism description
+int handle_sm_count(b200chem_handle h);
 
 bool rounds_supported(int N);
 RoundsSetupLayout rounds_setup_layout(int N, int R, int lut_bytes);

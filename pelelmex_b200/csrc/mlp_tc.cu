@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/b200chem.h"
+
 namespace b200 {
 namespace mlp {
 
@@ -52,6 +54,9 @@ struct GemmArgs {
   int* err;            // raised on an mbarrier timeout
   int vec_ok;          // C (and aux) rows 16-byte aligned: vector epilogue
   int stages;          // A stages of the warp-specialised kernel (<= kMaxStages)
+  int arep;            // A holds arep * K columns: arep BF16 terms of one K-wide operand
+                       // (hi, then lo), all multiplied by the same B and summed
+  int split_out;       // BF16 outputs as two terms: hi at column c, lo = bf16(v - hi) at c + N
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -274,7 +279,8 @@ __device__ __forceinline__ void epilogue_chunk(const GemmArgs& g, int row, int c
   } else {
     __nv_bfloat16* C = reinterpret_cast<__nv_bfloat16*>(g.C) + (long long)row * g.ldc + col0;
     if (g.epi == kEpiGeluBf16) {
-      float* P = g.aux ? g.aux + (long long)row * g.ldc + col0 : nullptr;
+      // pre-activations: row stride ldc, or N when C is written in two terms
+      float* P = g.aux ? g.aux + (long long)row * (g.split_out ? (long long)g.N : g.ldc) + col0 : nullptr;
       if (P && full) {
 #pragma unroll
         for (int q = 0; q < 8; ++q)
@@ -309,14 +315,34 @@ __device__ __forceinline__ void epilogue_chunk(const GemmArgs& g, int row, int c
       for (int q = 0; q < 16; ++q) {
         const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
         w[q] = *reinterpret_cast<const uint32_t*>(&b2);
+        if (g.split_out) {
+          // keep the rounding residual for the low term
+          const float2 hf = __bfloat1622float2(b2);
+          v[2 * q] -= hf.x;
+          v[2 * q + 1] -= hf.y;
+        }
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         reinterpret_cast<uint4*>(C)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+      if (g.split_out) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+          w[q] = *reinterpret_cast<const uint32_t*>(&b2);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          reinterpret_cast<uint4*>(C + g.N)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < 32; ++i)
-        if (col0 + i < g.n_valid) C[i] = __float2bfloat16_rn(v[i]);
+        if (col0 + i < g.n_valid) {
+          const __nv_bfloat16 hi = __float2bfloat16_rn(v[i]);
+          C[i] = hi;
+          if (g.split_out) C[g.N + i] = __float2bfloat16_rn(v[i] - __bfloat162float(hi));
+        }
     }
   }
 }
@@ -466,7 +492,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   const int NT = g.N;                       // one N tile (N <= 256)
   const int NT32 = (NT + 31) & ~31;         // accumulator 1 starts at column NT32
   const int KC = g.K <= 64 ? g.K : 64;      // K chunk of one stage
-  const int nchunk = g.K / KC;
+  const int nchunk = g.K * g.arep / KC;     // A chunks per tile (all terms)
+  const int bchunks = g.K / KC;             // B chunks (one term)
   unsigned char* Bs = smem;                                    // [K/8][NT][16 B]
   unsigned char* As = smem + ((NT * g.K * 2 + 1023) & ~1023);  // S x [KC/8][128][16 B]
   const int stage_bytes = kTileM * KC * 2;
@@ -538,7 +565,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           const uint32_t a0 = smem_u32(As + s * stage_bytes);
           for (int ks = 0; ks < KC / 16; ++ks) {
             const uint64_t ad = umma_desc(a0 + (uint32_t)(2 * ks) * a_lbo, a_lbo, 128u);
-            const uint64_t bd = umma_desc(b0 + (uint32_t)(c * (KC / 8) + 2 * ks) * b_lbo, b_lbo, 128u);
+            const uint64_t bd = umma_desc(b0 + (uint32_t)((c % bchunks) * (KC / 8) + 2 * ks) * b_lbo, b_lbo, 128u);
             umma_bf16(d, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
           }
           umma_commit(&sb.empty[s]);  // the stage is free once these MMAs have read it
@@ -607,6 +634,32 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   }
 }
 
+// Fused Adam step of one parameter tensor [rows][cols] (FP32 master copy),
+// Kingma & Ba 2015: m = b1 m + (1 - b1) g, v = b2 v + (1 - b2) g^2,
+// p -= lr (m / c1) / (sqrt(v / c2) + eps) with the bias corrections c1, c2;
+// then the BF16 copies the GEMMs read: wb (same layout) and wbt (transposed,
+// [cols][rows]), each optional.
+__global__ void adam_step(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, long long n, int cols, float lr, float b1, float b2, float eps,
+                          float c1, float c2, __nv_bfloat16* __restrict__ wb, __nv_bfloat16* __restrict__ wbt,
+                          int rows) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+    const __nv_bfloat16 b = __float2bfloat16_rn(pi);
+    if (wb) wb[i] = b;
+    if (wbt) {
+      const long long r = i / cols, c = i % cols;
+      wbt[c * rows + r] = b;
+    }
+  }
+}
+
 // Self-test of the bounded waits: one thread waits on an mbarrier that
 // nothing arrives at, with the same polling loop as the GEMM roles but a
 // caller-given bound, then raises the error flag and returns -- the path a
@@ -671,7 +724,13 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
                                       int* err, void* stream) {
   if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return -1;
   if (M % kTileM || N % 16 || K % 16 || (N > 256 && N % 256)) return -1;
+  const int arep = (epi & B200CHEM_GEMM_SPLIT_A) ? 2 : 1;
+  const int split_out = (epi & B200CHEM_GEMM_SPLIT_OUT) ? 1 : 0;
+  epi &= 0xF;
   if (epi < kEpiF32 || epi > kEpiDGeluBf16) return -1;
+  if (split_out && epi != kEpiBf16 && epi != kEpiGeluBf16) return -1;
+  if (split_out && (N > 256 || ldc < 2LL * N)) return -1;
+  if (lda < (long long)arep * K) return -1;
   if (epi == kEpiDGeluBf16 && !aux) return -1;
   if (lda % 8 || ldb % 8) return -1;  // 16-byte staging loads
   if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return -1;
@@ -690,10 +749,13 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
   g.epi = epi;
   g.n_valid = n_valid > 0 ? n_valid : N;
   g.err = err;
+  g.arep = arep;
+  g.split_out = split_out;
   {
     const size_t esz = (epi == kEpiF32) ? 4 : 2;
     const bool cal = (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ((ldc * (long long)esz) & 15) == 0;
-    const bool aal = !aux || ((reinterpret_cast<uintptr_t>(aux) & 15) == 0 && ((ldc * 4) & 15) == 0);
+    const long long ldaux = split_out ? N : ldc;
+    const bool aal = !aux || ((reinterpret_cast<uintptr_t>(aux) & 15) == 0 && ((ldaux * 4) & 15) == 0);
     g.vec_ok = (cal && aal) ? 1 : 0;
   }
   const bool resident = (K <= 256 && N <= 256);
@@ -704,7 +766,7 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
   if (resident && (K <= 64 || K % 64 == 0)) {
     // warp-specialised pipeline: TMA producer, MMA issuer, epilogue warps
     CUtensorMap ta, tb;
-    if (make_operand_map(&ta, A, K, M, lda, kTileM) || make_operand_map(&tb, B, K, N, ldb, N)) return -2;
+    if (make_operand_map(&ta, A, arep * K, M, lda, kTileM) || make_operand_map(&tb, B, K, N, ldb, N)) return -2;
     const int KC = K <= 64 ? K : 64;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -723,6 +785,7 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
     gemm_bf16_ws<<<grid, kWsThreads, smem, st>>>(g, ta, tb);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
   }
+  if (arep != 1) return -1;  // two-term A operands need the warp-specialised kernel
   const int NT = N <= 256 ? N : 256;
   const int KC = resident ? K : 64;
   const int smem = kTileM * KC * 2 + NT * KC * 2;
@@ -731,6 +794,18 @@ extern "C" int b200chem_mlp_gemm_bf16(const void* A, long long lda, const void* 
   const int tiles = (M / kTileM) * ((N + NT - 1) / NT);
   const int grid = tiles < sms ? tiles : sms;
   gemm_bf16_tc<<<grid, kThreads, smem, st>>>(g);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+extern "C" int b200chem_mlp_adam(float* p, const float* g, float* m, float* v, int rows, int cols, float lr,
+                                 float beta1, float beta2, float eps, int step, void* wb, void* wbt, void* stream) {
+  if (!p || !g || !m || !v || rows <= 0 || cols <= 0 || step < 1 || !(lr >= 0.0f)) return -1;
+  const long long n = (long long)rows * cols;
+  const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+  const long long blocks = (n + 255) / 256;
+  adam_step<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      p, g, m, v, n, cols, lr, beta1, beta2, eps, c1, c2, static_cast<__nv_bfloat16*>(wb),
+      static_cast<__nv_bfloat16*>(wbt), rows);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

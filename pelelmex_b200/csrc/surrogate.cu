@@ -1,36 +1,48 @@
 // surrogate.cu -- device side of the learned surrogate of the reaction
-// advance: network input features and the acceptance gate of a prediction.
+// advance and the hybrid reactor built on it.
 //
-// Network: N + 2 inputs (T, log10(Y_k + 1e-20) for the N species, log10 dt;
-// each standardised by the training-set mean and deviation, padded with
-// zeros to a multiple of 16 BF16 columns: 23 -> 32 for 21 species) -> 3 x 256
-// GELU -> N + 1 outputs (dT, dY_k, also standardised; 22 -> 32 columns).
-// The GEMMs run on the tensor cores (mlp_tc.cu).
+// Network (one ensemble member): N + 2 inputs (T, log10(Y_k + 1e-20) for the
+// N species, log10 dt; standardised by the training-set mean and deviation,
+// padded with zeros to a multiple of 16) -> 3 x 256 GELU -> N + 1 outputs
+// u_j, decoded as dy_j = s_j sinh(u_j ystd_j + ymean_j) (dT in K, dY_k).
+// Inputs and activations travel as two BF16 terms (hi, lo = bf16(v - hi));
+// the GEMMs are the tensor-core kernels of mlp_tc.cu.
 //
-// Gate, one thread per cell, in this order (any failure rejects the cell,
-// which then goes to the BDF integrator):
-//   0. (dT_max > 0) the predicted |dT| must not exceed dT_max: the surrogate
-//      is trusted where the chemistry over dt_react is mild;
-//   1. mass: the predicted partial densities z = rho0 (Y0 + dY) + dt extF_rhoY
-//      must sum to the target density within tol_mass (relative);
-//   2. element conservation: every element total sum_k a_ek z_k / W_k must
-//      match its target within tol_elem times the total atom content; then a
-//      weighted minimum-norm correction restores every element total exactly
-//      (weights max(|z_k|, 1e-10 rho), so trace species barely move), and
-//      partial densities below -tol_mass rho reject (smaller ones are clipped);
-//   3. energy consistency: rhoH1 = rhoH0 + dt extF_rhoH; T1 from (h1, Y1) by
-//      Newton from T0 + dT must agree with the predicted T0 + dT within tol_T
-//      (K); the accepted temperature is T1 (t_source 0: energy conserved
-//      exactly) or the predicted T0 + dT (t_source 1);
-//   4. one-step implicit residual (when rtol > 0): r = y1 - y0 - dt/2 (f(y0) +
-//      f(y1)) (trapezoidal rule, the second-order one-step implicit member),
-//      max_i |r_i| / (rtol |y1_i| + atol s_i + rchange |y1_i - y0_i|) <= 1
-//      with scales s = rho0 for species and T0 for the temperature, over all
-//      components or (residual_t_only) the temperature alone.
-// Accepted cells get rhoY1, T1, rhoH1 and fctCount (right-hand sides used:
-// 2 with the residual check, else 0) written in place.
+// Hybrid react (b200chem_react_hybrid), per chunk of cells:
+//   1. features of every cell (two-term BF16);
+//   2. the four GEMMs of every member (FP32 predictions);
+//   3. the gate, one thread per cell (hy_gate), in this order:
+//        spread   every member's dT within `spread` bars of the ensemble mean
+//                 (a bar is t_rel * T1, the error allowed to the cell);
+//        cap      |mean dT| within `dT_cap` bars: the members share a bias of
+//                 a few percent of the change, which their spread cannot see,
+//                 so agreement bounds the error only for moderate changes;
+//        mass     the predicted partial densities z = rho0 (Y0 + dY) + dt F
+//                 sum to the target density within tol_mass;
+//        elements every element total within tol_elem of its target;
+//        energy   T from (h1, Y(z)) within `gap` bars of T1 = T0 + dT, with
+//                 rhoH1 = rhoH0 + dt F_H;
+//        project  weighted minimum-norm correction of z onto the element
+//                 totals and the energy rhoH1 = sum_k h_k(T1) z_k (weights
+//                 max(|z_k|, 1e-10 rho): trace species barely move), so the
+//                 accepted state conserves elements and energy exactly and
+//                 its T is the one (h1, Y) gives; partial densities below
+//                 -tol_mass rho reject, smaller ones are clipped;
+//        residual (resid > 0) |T1 - T0 - dt/2 (f_T(y0) + f_T(y1))| within
+//                 `resid` bars (two right-hand sides; the one-step implicit
+//                 trapezoidal relation of the temperature);
+//      accepted cells are written in place; the others are appended to a
+//      list (warp-aggregated);
+//   4. the listed cells are gathered into compact arrays, integrated by the
+//      BDF (b200chem_react_flat), and scattered back.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
 
 #include "bdf_thread.cuh"
 #include "common.cuh"
@@ -43,248 +55,58 @@ namespace {
 constexpr int sg_in(int N) { return (N + 2 + 15) / 16 * 16; }
 constexpr int sg_out(int N) { return (N + 1 + 15) / 16 * 16; }
 constexpr int kSgBlock = 64;
+constexpr int kHidden = 256;
+constexpr int kMaxMembers = 16;
+constexpr int kMaxElem = 8;
 
 struct FeatParams {
-  const double* rhoY;  // [N][ncells]
+  const double* rhoY;  // [N][ld] (cells c0 .. c0 + ncells - 1 used)
   const double* T;
+  long long ld;        // component stride of rhoY
+  long long c0;        // first cell
   long long ncells, nrows;  // nrows: padded to a multiple of 128
   double log10dt;
   const float* xmean;  // [N + 2]
   const float* xstd;
-  __nv_bfloat16* x;    // [nrows][32]
+  __nv_bfloat16* x;    // [nrows][terms * in]
+  int terms;           // 1: bf16(x); 2: [bf16(x) | bf16(x - bf16(x))]
 };
 
 template <int NS>
 __global__ void __launch_bounds__(128) sg_features(FeatParams P) {
   constexpr int kSgIn = sg_in(NS);
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.nrows;
-       c += (long long)gridDim.x * blockDim.x) {
-    __align__(16) __nv_bfloat16 row[kSgIn];
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nrows;
+       r += (long long)gridDim.x * blockDim.x) {
+    float xv[kSgIn];
 #pragma unroll
-    for (int j = 0; j < kSgIn; ++j) row[j] = __float2bfloat16_rn(0.0f);
-    if (c < P.ncells) {
+    for (int j = 0; j < kSgIn; ++j) xv[j] = 0.0f;
+    if (r < P.ncells) {
+      const long long c = P.c0 + r;
       double rho = 0.0;
 #pragma unroll 4
-      for (int k = 0; k < NS; ++k) rho += P.rhoY[(long long)k * P.ncells + c];
+      for (int k = 0; k < NS; ++k) rho += P.rhoY[(long long)k * P.ld + c];
       const double rinv = 1.0 / rho;
-      row[0] = __float2bfloat16_rn((float)((P.T[c] - P.xmean[0]) / P.xstd[0]));
+      xv[0] = (float)((P.T[c] - P.xmean[0]) / P.xstd[0]);
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
-        const double Y = P.rhoY[(long long)k * P.ncells + c] * rinv;
+        const double Y = P.rhoY[(long long)k * P.ld + c] * rinv;
         const double f = log10(fmax(Y, 0.0) + 1e-20);
-        row[1 + k] = __float2bfloat16_rn((float)((f - P.xmean[1 + k]) / P.xstd[1 + k]));
+        xv[1 + k] = (float)((f - P.xmean[1 + k]) / P.xstd[1 + k]);
       }
-      row[NS + 1] = __float2bfloat16_rn((float)((P.log10dt - P.xmean[NS + 1]) / P.xstd[NS + 1]));
+      xv[NS + 1] = (float)((P.log10dt - P.xmean[NS + 1]) / P.xstd[NS + 1]);
     }
-    uint4* dst = reinterpret_cast<uint4*>(P.x + c * kSgIn);
-    const uint4* src = reinterpret_cast<const uint4*>(row);
+    __align__(16) __nv_bfloat16 row[kSgIn];
+    uint4* dst = reinterpret_cast<uint4*>(P.x + r * kSgIn * P.terms);
+    for (int t = 0; t < P.terms; ++t) {
 #pragma unroll
-    for (int q = 0; q < kSgIn * 2 / 16; ++q) dst[q] = src[q];
-  }
-}
-
-struct GateParams {
-  DevMech mech;
-  double* rhoY;  // [N][ncells] in/out
-  const double* fY;
-  double* T;
-  double* rhoH;
-  const double* fH;
-  double* fct;   // may be null
-  long long ncells;
-  double dt;
-  const float* pred;  // [nrows][32] standardised network outputs
-  const float* ymean;  // [N + 1]
-  const float* ystd;
-  const double* elem;  // [ne][N] atoms per species
-  int ne;
-  b200chem_gate_opts o;
-  int* accept;   // [ncells] 1 accepted, else -(first failed check): 1 mass, 2 elements, 3 energy,
-                 // 4 residual, 5 change cap
-};
-
-template <int NS>
-__global__ void __launch_bounds__(kSgBlock) sg_gate(GateParams P) {
-  constexpr int n = NS + 1;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  __shared__ DevMech s_mech;
-  if (threadIdx.x == 0) s_mech = P.mech;
-  __syncthreads();
-  const DevMech& m = s_mech;
-  double* sC = reinterpret_cast<double*>(dsm) + threadIdx.x;
-  double* sW = sC + NS * blockDim.x;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.ncells;
-       c += (long long)gridDim.x * blockDim.x) {
-    double y0[n], y1[n], F[n], f0[n], f1[n];
-    double rho0 = 0.0;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      y0[k] = P.rhoY[(long long)k * P.ncells + c];
-      F[k] = P.fY[(long long)k * P.ncells + c];
-      rho0 += y0[k];
-    }
-    y0[NS] = P.T[c];
-    F[NS] = P.fH[c];
-    const float* pr = P.pred + c * sg_out(NS);
-    const double dT = (double)pr[0] * P.ystd[0] + P.ymean[0];
-    bool ok = rho0 > 0.0 && y0[NS] > 0.0 && isfinite(dT);
-    int stage = ok ? 0 : 1;  // first failed check (0: none)
-    if (ok && P.o.dT_max > 0.0 && fabs(dT) > P.o.dT_max) {
-      ok = false;
-      stage = 5;
-    }
-    // predicted partial densities z = rho0 Y1 + dt extF_rhoY and their targets
-    double rho1t = 0.0;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      const double Y = y0[k] / rho0 + ((double)pr[1 + k] * P.ystd[1 + k] + P.ymean[1 + k]);
-      y1[k] = rho0 * Y + P.dt * F[k];
-      rho1t += y0[k] + P.dt * F[k];
-      if (!isfinite(y1[k])) ok = false;
-    }
-    // 1. mass, before any correction
-    if (ok) {
-      double zs = 0.0;
-#pragma unroll
-      for (int k = 0; k < NS; ++k) zs += y1[k];
-      ok = fabs(zs - rho1t) <= P.o.tol_mass * rho1t;
-      if (!ok) stage = 1;
-    }
-    // 2. elements, before any correction; then the weighted minimum-norm
-    //    correction that restores every element total exactly:
-    //    z' = z - D C^T (C D C^T)^-1 (C z - c), C[e][k] = a_ek / W_k,
-    //    D = diag(max(|z_k|, 1e-10 rho)) (trace species barely move)
-    constexpr int kMaxE = 8;
-    if (ok && P.ne > 0) {
-      const int ne = P.ne < kMaxE ? P.ne : kMaxE;
-      double res[kMaxE], G[kMaxE][kMaxE];
-      double tot = 0.0, worst = 0.0;
-      for (int e = 0; e < ne; ++e) {
-        double ct = 0.0, cz = 0.0;
-#pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          const double a = __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k);
-          ct += a * (y0[k] + P.dt * F[k]);
-          cz += a * y1[k];
-        }
-        res[e] = cz - ct;
-        tot += ct;
-        worst = fmax(worst, fabs(res[e]));
-        for (int f = 0; f < ne; ++f) {
-          double g = 0.0;
-#pragma unroll
-          for (int k = 0; k < NS; ++k)
-            g += __ldg(P.elem + e * NS + k) * __ldg(P.elem + f * NS + k) * __ldg(m.inv_mw + k) *
-                 __ldg(m.inv_mw + k) * fmax(fabs(y1[k]), 1e-10 * rho0);
-          G[e][f] = g;
-        }
+      for (int j = 0; j < kSgIn; ++j) {
+        row[j] = __float2bfloat16_rn(xv[j]);
+        xv[j] -= __bfloat162float(row[j]);  // residual for the next term
       }
-      ok = worst <= P.o.tol_elem * tot;
-      if (!ok) stage = 2;
-      if (ok) {
-        // solve G lam = res (Gauss-Jordan with partial pivoting; elements
-        // absent from the mechanism give a zero row and are skipped)
-        double lam[kMaxE];
-        int perm[kMaxE];
-        for (int e = 0; e < ne; ++e) perm[e] = e;
-        for (int e = 0; e < ne; ++e) lam[e] = res[e];
-        for (int col = 0; col < ne; ++col) {
-          int piv = col;
-          for (int r = col + 1; r < ne; ++r)
-            if (fabs(G[r][col]) > fabs(G[piv][col])) piv = r;
-          if (!(fabs(G[piv][col]) > 0.0)) continue;
-          if (piv != col) {
-            for (int q = 0; q < ne; ++q) {
-              const double t = G[col][q];
-              G[col][q] = G[piv][q];
-              G[piv][q] = t;
-            }
-            const double t = lam[col];
-            lam[col] = lam[piv];
-            lam[piv] = t;
-          }
-          const double inv = 1.0 / G[col][col];
-          for (int r = 0; r < ne; ++r) {
-            if (r == col) continue;
-            const double f = G[r][col] * inv;
-            if (f == 0.0) continue;
-            for (int q = col; q < ne; ++q) G[r][q] -= f * G[col][q];
-            lam[r] -= f * lam[col];
-          }
-        }
-        for (int e = 0; e < ne; ++e) lam[e] = (fabs(G[e][e]) > 0.0) ? lam[e] / G[e][e] : 0.0;
-        (void)perm;
+      const uint4* src = reinterpret_cast<const uint4*>(row);
 #pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          double corr = 0.0;
-          for (int e = 0; e < ne; ++e) corr += __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) * lam[e];
-          y1[k] -= fmax(fabs(y1[k]), 1e-10 * rho0) * corr;
-        }
-      }
+      for (int q = 0; q < kSgIn * 2 / 16; ++q) dst[t * (kSgIn * 2 / 16) + q] = src[q];
     }
-    // negative partial densities: small ones are clipped, larger ones reject
-    if (ok) {
-#pragma unroll
-      for (int k = 0; k < NS; ++k) {
-        if (y1[k] < -P.o.tol_mass * rho1t) ok = false;
-        y1[k] = fmax(y1[k], 0.0);
-      }
-      if (!ok) stage = 1;
-    }
-    // 3. energy: T1 from (h1, Y1) by Newton from T0 + dT must agree with T0 + dT
-    double rho1 = 0.0;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) rho1 += y1[k];
-    const double rhoH1 = P.rhoH[c] + P.dt * F[NS];
-    if (ok) {
-      const double h1 = rhoH1 / rho1;
-      double T = y0[NS] + dT;
-      bool conv = false;
-      for (int it = 0; it < 50 && T > 0.0; ++it) {
-        const double lnT = log(T);
-        double hs = 0.0, cs = 0.0;
-#pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          double cpR, hRT, sR, dcpR;
-          nasa7(m, k, T, lnT, cpR, hRT, sR, dcpR);
-          const double w = y1[k] / rho1 * __ldg(m.inv_mw + k) * kRu;
-          hs += w * hRT * T;
-          cs += w * cpR;
-        }
-        const double dTn = (h1 - hs) / cs;
-        T += dTn;
-        if (fabs(dTn) <= 1e-10 * T) {
-          conv = true;
-          break;
-        }
-      }
-      ok = conv && fabs(T - (y0[NS] + dT)) <= P.o.tol_T;
-      y1[NS] = P.o.t_source ? y0[NS] + dT : T;
-      if (!ok) stage = 3;
-    }
-    // 4. one-step implicit residual (rtol <= 0 switches it off)
-    if (ok && P.o.rtol > 0.0) {
-      tpc::tpc_rhs<NS>(m, y0, F, f0, sC, sW, blockDim.x);
-      tpc::tpc_rhs<NS>(m, y1, F, f1, sC, sW, blockDim.x);
-      double worst = 0.0;
-#pragma unroll
-      for (int i = 0; i < n; ++i) {
-        if (P.o.residual_t_only && i < NS) continue;
-        const double r = y1[i] - y0[i] - 0.5 * P.dt * (f0[i] + f1[i]);
-        const double sc = (i < NS) ? rho0 : y0[NS];
-        worst = fmax(worst, fabs(r) / (P.o.rtol * fabs(y1[i]) + P.o.atol * sc + P.o.rchange * fabs(y1[i] - y0[i])));
-      }
-      ok = worst <= 1.0;
-      if (!ok) stage = 4;
-    }
-    if (ok) {
-#pragma unroll
-      for (int k = 0; k < NS; ++k) P.rhoY[(long long)k * P.ncells + c] = y1[k];
-      P.T[c] = y1[NS];
-      P.rhoH[c] = rhoH1;
-      if (P.fct) P.fct[c] = (P.o.rtol > 0.0) ? 2.0 : 0.0;
-    }
-    P.accept[c] = ok ? 1 : -stage;
   }
 }
 
@@ -295,14 +117,388 @@ int launch_features(const FeatParams& P, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? 0 : B200CHEM_ECUDA;
 }
 
+int features_for(int N, const FeatParams& P, cudaStream_t st) {
+  switch (N) {
+    case 9: return launch_features<9>(P, st);
+    case 21: return launch_features<21>(P, st);
+    case 53: return launch_features<53>(P, st);
+    default: return B200CHEM_EINVAL;
+  }
+}
+
+// ------------------------------------------------------------------ gate
+enum GateReason : int {
+  kAccept = 0,
+  kRejSpread = 1,
+  kRejCap = 2,
+  kRejMass = 3,
+  kRejElem = 4,
+  kRejEnergy = 5,
+  kRejNegative = 6,
+  kRejResid = 7,
+  kRejNonfinite = 8,
+  kReasons = 9
+};
+
+struct GateParams {
+  DevMech mech;
+  double* rhoY;  // [N][ld] in/out
+  const double* fY;
+  double* T;
+  double* rhoH;
+  const double* fH;
+  double* fct;          // may be null
+  const int* mask;      // may be null
+  int* status;          // may be null
+  long long ld;         // component stride of the state arrays (all cells)
+  long long c0, nc;     // cells c0 .. c0 + nc - 1 of this chunk
+  double dt;
+  const float* pred;    // [M][rows][kout] standardised outputs of every member
+  long long rows;       // rows of one member's prediction block
+  int members;
+  const float* ymean;   // [N + 1]
+  const float* ystd;
+  const double* tscale; // [N + 1] asinh scales
+  const double* elem;   // [ne][N] atoms of each element in each species
+  int ne;
+  b200chem_hybrid_opts o;
+  int* rej_list;        // rejected cells (global indices)
+  int* rej_count;
+  unsigned long long* reasons;  // [kReasons] counts (kAccept: accepted)
+};
+
+// T from (h, Y) by Newton on sum_k Y_k h_k(T) = h, from T; false when it
+// does not converge to 1e-10 relative in 50 iterations.
 template <int NS>
-int launch_gate(const GateParams& P, cudaStream_t st) {
+__device__ bool t_from_h(const DevMech& m, double h, const double* z, double rho, double& T) {
+  for (int it = 0; it < 50 && T > 0.0; ++it) {
+    const double lnT = log(T);
+    double hs = 0.0, cs = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < NS; ++k) {
+      double cpR, hRT, sR, dcpR;
+      nasa7(m, k, T, lnT, cpR, hRT, sR, dcpR);
+      const double w = z[k] / rho * __ldg(m.inv_mw + k) * kRu;
+      hs += w * hRT * T;
+      cs += w * cpR;
+    }
+    const double dTn = (h - hs) / cs;
+    T += dTn;
+    if (fabs(dTn) <= 1e-10 * T) return true;
+  }
+  return false;
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
+  constexpr int n = NS + 1;
+  constexpr int kout = sg_out(NS);
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ DevMech s_mech;
+  if (threadIdx.x == 0) s_mech = P.mech;
+  __syncthreads();
+  const DevMech& m = s_mech;
+  double* sC = reinterpret_cast<double*>(dsm) + threadIdx.x;
+  double* sW = sC + NS * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  // warp-uniform trip count: every lane of a warp runs the same iterations
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < P.nc; base += (long long)gridDim.x * blockDim.x) {
+    const long long r = base + threadIdx.x;
+    const bool in = r < P.nc;
+    const long long c = P.c0 + r;
+    int reason = kAccept;
+    const bool masked = in && P.mask && P.mask[c] == 0;
+    if (in && !masked) {
+      double y0[n], F[n], d[n], z[NS];
+      double rho0 = 0.0;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        y0[k] = P.rhoY[(long long)k * P.ld + c];
+        F[k] = P.fY[(long long)k * P.ld + c];
+        rho0 += y0[k];
+      }
+      y0[NS] = P.T[c];
+      F[NS] = P.fH[c];
+      // ensemble mean of the decoded changes, and the extremes of dT
+#pragma unroll
+      for (int j = 0; j < n; ++j) d[j] = 0.0;
+      double tmin = 1e300, tmax = -1e300;
+      for (int mb = 0; mb < P.members; ++mb) {
+        const float* pr = P.pred + ((long long)mb * P.rows + r) * kout;
+#pragma unroll
+        for (int j = 0; j < n; ++j) {
+          const double u = (double)pr[j] * (double)P.ystd[j] + (double)P.ymean[j];
+          const double v = P.tscale[j] * sinh(u);
+          d[j] += v;
+          if (j == 0) {
+            tmin = fmin(tmin, v);
+            tmax = fmax(tmax, v);
+          }
+        }
+      }
+      const double invM = 1.0 / P.members;
+#pragma unroll
+      for (int j = 0; j < n; ++j) d[j] *= invM;
+      const double dT = d[0];
+      const double T0 = y0[NS];
+      const double T1 = T0 + dT;
+      const double bar = P.o.t_rel * T1;  // the error allowed to this cell, K
+      const bool fin = rho0 > 0.0 && T0 > 0.0 && isfinite(dT) && T1 > 0.0;
+      if (!fin) reason = kRejNonfinite;
+      if (!reason && fmax(tmax - dT, dT - tmin) > P.o.spread * bar) reason = kRejSpread;
+      if (!reason && fabs(dT) > P.o.dT_cap * bar) reason = kRejCap;
+      // predicted partial densities and their targets
+      double rho1t = 0.0;
+      if (!reason) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          z[k] = rho0 * (y0[k] / rho0 + d[1 + k]) + P.dt * F[k];
+          rho1t += y0[k] + P.dt * F[k];
+          if (!isfinite(z[k])) reason = kRejNonfinite;
+        }
+      }
+      if (!reason) {
+        double zs = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) zs += z[k];
+        if (!(fabs(zs - rho1t) <= P.o.tol_mass * rho1t)) reason = kRejMass;
+      }
+      // constraint rows: the elements (mol of element per gram of species),
+      // then the energy at T1 (erg per gram), each scaled to unit max-norm
+      const int ne = P.ne < kMaxElem ? P.ne : kMaxElem;
+      double res[kMaxElem + 1], rsc[kMaxElem + 1];
+      double hk[NS];
+      const double rhoH1 = P.rhoH[c] + P.dt * F[NS];
+      if (!reason) {
+        double tot = 0.0, worst = 0.0;
+        for (int e = 0; e < ne; ++e) {
+          double ct = 0.0, cz = 0.0, mx = 0.0;
+#pragma unroll
+          for (int k = 0; k < NS; ++k) {
+            const double a = __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k);
+            ct += a * (y0[k] + P.dt * F[k]);
+            cz += a * z[k];
+            mx = fmax(mx, fabs(a));
+          }
+          res[e] = cz - ct;
+          rsc[e] = mx > 0.0 ? 1.0 / mx : 0.0;
+          tot += ct;
+          worst = fmax(worst, fabs(res[e]));
+        }
+        if (!(worst <= P.o.tol_elem * tot)) reason = kRejElem;
+      }
+      if (!reason) {
+        // energy consistency of the raw prediction: T(h1, Y(z)) against T1
+        double zc[NS];
+        double zsum = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          zc[k] = fmax(z[k], 0.0);
+          zsum += zc[k];
+        }
+        double Th = T1;
+        const bool conv = t_from_h<NS>(m, rhoH1 / zsum, zc, zsum, Th);
+        if (!conv || !(fabs(Th - T1) <= P.o.gap * bar)) reason = kRejEnergy;
+      }
+      if (!reason) {
+        // species enthalpies at T1 and the energy row
+        const double lnT1 = log(T1);
+        double ez = 0.0, mx = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          double cpR, hRT, sR, dcpR;
+          nasa7(m, k, T1, lnT1, cpR, hRT, sR, dcpR);
+          hk[k] = hRT * kRu * T1 * __ldg(m.inv_mw + k);
+          ez += hk[k] * z[k];
+          mx = fmax(mx, fabs(hk[k]));
+        }
+        res[ne] = ez - rhoH1;
+        rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
+        // weighted minimum-norm correction: z' = z - D A^T (A D A^T)^-1 (A z - b)
+        // over the ne + 1 scaled rows A (zero rows are skipped)
+        const int nr = ne + 1;
+        double G[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
+        auto row = [&](int e, int k) -> double {
+          return (e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k]) * rsc[e];
+        };
+        for (int e = 0; e < nr; ++e) {
+          lam[e] = res[e] * rsc[e];
+          for (int f = 0; f < nr; ++f) {
+            double g = 0.0;
+            for (int k = 0; k < NS; ++k) g += row(e, k) * row(f, k) * fmax(fabs(z[k]), 1e-10 * rho0);
+            G[e][f] = g;
+          }
+        }
+        // Gauss-Jordan with partial pivoting (singular pivots: row skipped)
+        for (int col = 0; col < nr; ++col) {
+          int piv = col;
+          for (int w = col + 1; w < nr; ++w)
+            if (fabs(G[w][col]) > fabs(G[piv][col])) piv = w;
+          if (!(fabs(G[piv][col]) > 1e-300)) continue;
+          if (piv != col) {
+            for (int w = 0; w < nr; ++w) {
+              const double t = G[col][w];
+              G[col][w] = G[piv][w];
+              G[piv][w] = t;
+            }
+            const double t = lam[col];
+            lam[col] = lam[piv];
+            lam[piv] = t;
+          }
+          const double inv = 1.0 / G[col][col];
+          for (int w = 0; w < nr; ++w) {
+            if (w == col) continue;
+            const double f = G[w][col] * inv;
+            if (f == 0.0) continue;
+            for (int v = col; v < nr; ++v) G[w][v] -= f * G[col][v];
+            lam[w] -= f * lam[col];
+          }
+        }
+        for (int e = 0; e < nr; ++e) lam[e] = (fabs(G[e][e]) > 1e-300) ? lam[e] / G[e][e] : 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          double corr = 0.0;
+          for (int e = 0; e < nr; ++e) corr += row(e, k) * lam[e];
+          z[k] -= fmax(fabs(z[k]), 1e-10 * rho0) * corr;
+        }
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          if (z[k] < -P.o.tol_mass * rho1t) reason = kRejNegative;
+          z[k] = fmax(z[k], 0.0);
+        }
+      }
+      if (!reason && P.o.resid > 0.0) {
+        double y1[n], f0[n], f1[n];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) y1[k] = z[k];
+        y1[NS] = T1;
+        tpc::tpc_rhs<NS>(m, y0, F, f0, sC, sW, blockDim.x);
+        tpc::tpc_rhs<NS>(m, y1, F, f1, sC, sW, blockDim.x);
+        const double rT = T1 - T0 - 0.5 * P.dt * (f0[NS] + f1[NS]);
+        if (!(fabs(rT) <= P.o.resid * bar)) reason = kRejResid;
+      }
+      if (!reason) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) P.rhoY[(long long)k * P.ld + c] = z[k];
+        P.T[c] = T1;
+        P.rhoH[c] = rhoH1;
+        if (P.fct) P.fct[c] = (P.o.resid > 0.0) ? 2.0 : 0.0;
+        if (P.status) P.status[c] = B200CHEM_CELL_OK;
+      }
+    } else if (masked) {
+      if (P.fct) P.fct[c] = 0.0;
+      if (P.status) P.status[c] = B200CHEM_CELL_MASKED;
+    }
+    // rejected cells: warp-aggregated append to the list
+    const bool rej = in && !masked && reason != kAccept;
+    const unsigned bal = __ballot_sync(0xffffffffu, rej);
+    if (bal) {
+      int basei = 0;
+      if (lane == 0) basei = atomicAdd(P.rej_count, __popc(bal));
+      basei = __shfl_sync(0xffffffffu, basei, 0);
+      if (rej) P.rej_list[basei + __popc(bal & ((1u << lane) - 1u))] = (int)c;
+    }
+    // per-reason counts, one atomic per warp and reason present
+#pragma unroll
+    for (int q = 0; q < kReasons; ++q) {
+      const unsigned b = __ballot_sync(0xffffffffu, in && !masked && reason == q);
+      if (b && lane == 0) atomicAdd(P.reasons + q, (unsigned long long)__popc(b));
+    }
+  }
+}
+
+template <int NS>
+int launch_gate(const GateParams& P, int sm_count, cudaStream_t st) {
   const int smem = 2 * NS * kSgBlock * (int)sizeof(double);
-  if (cudaFuncSetAttribute(sg_gate<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(hy_gate<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return B200CHEM_ECUDA;
-  const long long blocks = (P.ncells + kSgBlock - 1) / kSgBlock;
-  sg_gate<NS><<<(unsigned)(blocks < 65535 ? blocks : 65535), kSgBlock, smem, st>>>(P);
+  const long long need = (P.nc + kSgBlock - 1) / kSgBlock;
+  const long long cap = 16LL * sm_count;
+  hy_gate<NS><<<(unsigned)(need < cap ? need : cap), kSgBlock, smem, st>>>(P);
   return cudaGetLastError() == cudaSuccess ? 0 : B200CHEM_ECUDA;
+}
+
+int gate_for(int N, const GateParams& P, int sm_count, cudaStream_t st) {
+  switch (N) {
+    case 9: return launch_gate<9>(P, sm_count, st);
+    case 21: return launch_gate<21>(P, sm_count, st);
+    case 53: return launch_gate<53>(P, sm_count, st);
+    default: return B200CHEM_EINVAL;
+  }
+}
+
+// ----------------------------------------------- gather / scatter / decode
+struct MoveParams {
+  const int* list;
+  const int* count;
+  int N;
+  long long ld;      // component stride of the full arrays
+  long long cap;     // component stride of the compact arrays
+  double *rhoY, *T, *rhoH, *fct;
+  const double *fY, *fH;
+  int* status;
+  double *cY, *cT, *cH, *cfY, *cfH, *cfct;
+  int* cstatus;
+};
+
+__global__ void hy_gather(MoveParams P) {
+  const int cnt = *P.count;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const long long c = P.list[i];
+    for (int k = 0; k < P.N; ++k) {
+      P.cY[k * P.cap + i] = P.rhoY[k * P.ld + c];
+      P.cfY[k * P.cap + i] = P.fY[k * P.ld + c];
+    }
+    P.cT[i] = P.T[c];
+    P.cH[i] = P.rhoH[c];
+    P.cfH[i] = P.fH[c];
+  }
+}
+
+__global__ void hy_scatter(MoveParams P, double fct_extra) {
+  const int cnt = *P.count;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const long long c = P.list[i];
+    for (int k = 0; k < P.N; ++k) P.rhoY[k * P.ld + c] = P.cY[k * P.cap + i];
+    P.T[c] = P.cT[i];
+    P.rhoH[c] = P.cH[i];
+    if (P.fct) P.fct[c] = P.cfct[i] + fct_extra;
+    if (P.status) P.status[c] = P.cstatus[i];
+  }
+}
+
+// Ensemble mean of the decoded changes [ncells][N + 1] and the largest
+// deviation of a member's dT from it [ncells].
+struct DecodeParams {
+  const float* pred;
+  long long rows, c0, nc;
+  int members, nout, kout;
+  const float *ymean, *ystd;
+  const double* tscale;
+  double* mean;    // [ncells_total][nout], rows c0..
+  double* spread;  // [ncells_total] (may be null)
+};
+
+__global__ void hy_decode(DecodeParams P) {
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nc; r += (long long)gridDim.x * blockDim.x) {
+    double tmin = 1e300, tmax = -1e300, tmean = 0.0;
+    for (int j = 0; j < P.nout; ++j) {
+      double s = 0.0;
+      for (int mb = 0; mb < P.members; ++mb) {
+        const double u = (double)P.pred[((long long)mb * P.rows + r) * P.kout + j] * (double)P.ystd[j] + P.ymean[j];
+        const double v = P.tscale[j] * sinh(u);
+        s += v;
+        if (j == 0) {
+          tmin = fmin(tmin, v);
+          tmax = fmax(tmax, v);
+        }
+      }
+      s /= P.members;
+      if (j == 0) tmean = s;
+      P.mean[(P.c0 + r) * P.nout + j] = s;
+    }
+    if (P.spread) P.spread[P.c0 + r] = fmax(tmax - tmean, tmean - tmin);
+  }
 }
 
 }  // namespace
@@ -310,63 +506,464 @@ int launch_gate(const GateParams& P, cudaStream_t st) {
 
 using namespace b200;
 
-extern "C" int b200chem_surrogate_features(b200chem_handle h, const double* rhoY, const double* T, int64_t ncells,
-                                           int64_t nrows, double dt, const float* xmean, const float* xstd,
-                                           void* x_bf16, void* stream) {
-  if (!h || ncells < 0 || nrows < ncells || nrows % 128 || !(dt > 0.0) || !xmean || !xstd || !x_bf16)
-    return handle_set_error(B200CHEM_EINVAL, "surrogate_features: bad arguments");
-  if (ncells > 0 && (!rhoY || !T)) return handle_set_error(B200CHEM_EINVAL, "surrogate_features: null state");
-  FeatParams P{rhoY, T, ncells, nrows, log10(dt), xmean, xstd, static_cast<__nv_bfloat16*>(x_bf16)};
-  const cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int err;
-  switch (handle_species(h)) {
-    case 9: err = launch_features<9>(P, st); break;
-    case 21: err = launch_features<21>(P, st); break;
-    case 53: err = launch_features<53>(P, st); break;
-    default: return handle_set_error(B200CHEM_EINVAL, "surrogate not compiled for this species count");
+// ------------------------------------------------------- surrogate object
+struct b200chem_surrogate {
+  b200chem_handle h = nullptr;
+  int device = -1;
+  int N = 0, nin = 0, nout = 0, kin = 0, kout = 0, members = 0, terms = 0, ne = 0;
+  b200chem_hybrid_opts opts{};
+  void* d_params = nullptr;  // normalisation, scales, elements, weights (one allocation)
+  const float *xmean = nullptr, *xstd = nullptr, *ymean = nullptr, *ystd = nullptr;
+  const double* tscale = nullptr;
+  const double* elem = nullptr;
+  std::vector<const void*> W;   // [members * 4] BF16 weights
+  std::vector<const float*> b;  // [members * 4] FP32 biases
+  void* d_scratch = nullptr;    // inference scratch (grown on demand)
+  size_t scratch_bytes = 0;
+  void* d_hy = nullptr;         // hybrid scratch: reject list, counters, compact state
+  size_t hy_bytes = 0;
+  int* h_count = nullptr;       // pinned: rejected count, GEMM error flag
+  cudaStream_t last_stream = nullptr;
+};
+
+namespace {
+
+constexpr char kMagic[8] = {'B', '2', 'C', 'H', 'S', 'U', 'R', 'R'};
+constexpr uint32_t kFileVersion = 1;
+constexpr long long kChunkRows = 1LL << 20;
+
+int sur_err(int code, const char* msg) { return handle_set_error(code, msg); }
+
+#define SCK(x)                                                        \
+  do {                                                                \
+    cudaError_t e_ = (x);                                             \
+    if (e_ != cudaSuccess) {                                          \
+      char m_[256];                                                   \
+      snprintf(m_, sizeof(m_), "%s: %s", #x, cudaGetErrorString(e_)); \
+      return sur_err(B200CHEM_ECUDA, m_);                             \
+    }                                                                 \
+  } while (0)
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Inference scratch for chunks of `rows` rows: x [rows][terms * kin] BF16,
+// two activation buffers [rows][terms * 256] BF16, predictions
+// [members][rows][kout] FP32, and the GEMM error flag.
+struct InferBufs {
+  __nv_bfloat16* x;
+  __nv_bfloat16* h0;
+  __nv_bfloat16* h1;
+  float* pred;
+  int* err;
+};
+
+size_t infer_bytes(const b200chem_surrogate* s, long long rows) {
+  return align256((size_t)rows * s->terms * s->kin * 2) + 2 * align256((size_t)rows * s->terms * kHidden * 2) +
+         align256((size_t)s->members * rows * s->kout * 4) + 256;
+}
+
+int ensure_infer(b200chem_surrogate* s, long long rows, cudaStream_t st, InferBufs* B) {
+  const size_t need = infer_bytes(s, rows);
+  if (need > s->scratch_bytes) {
+    if (s->d_scratch) {
+      SCK(cudaStreamSynchronize(st));
+      cudaFree(s->d_scratch);
+      s->d_scratch = nullptr;
+      s->scratch_bytes = 0;
+    }
+    if (cudaMalloc(&s->d_scratch, need) != cudaSuccess) {
+      cudaGetLastError();
+      return sur_err(B200CHEM_ENOMEM, "cannot allocate the surrogate's inference scratch");
+    }
+    s->scratch_bytes = need;
   }
-  if (err) return handle_set_error(err, "surrogate_features: launch failed");
-  handle_count_launch(h);
+  unsigned char* p = static_cast<unsigned char*>(s->d_scratch);
+  B->x = reinterpret_cast<__nv_bfloat16*>(p);
+  p += align256((size_t)rows * s->terms * s->kin * 2);
+  B->h0 = reinterpret_cast<__nv_bfloat16*>(p);
+  p += align256((size_t)rows * s->terms * kHidden * 2);
+  B->h1 = reinterpret_cast<__nv_bfloat16*>(p);
+  p += align256((size_t)rows * s->terms * kHidden * 2);
+  B->pred = reinterpret_cast<float*>(p);
+  p += align256((size_t)s->members * rows * s->kout * 4);
+  B->err = reinterpret_cast<int*>(p);
   return 0;
 }
 
-extern "C" int b200chem_surrogate_gate(b200chem_handle h, double* rhoY, const double* extF_rhoY, double* T,
-                                       double* rhoH, const double* extF_rhoH, double* fctCount, int64_t ncells,
-                                       double dt, const float* pred, const float* ymean, const float* ystd,
-                                       const double* elem, int32_t n_elements, const b200chem_gate_opts* opts,
-                                       int32_t* accept, void* stream) {
-  if (!h || ncells < 0 || !(dt > 0.0) || !opts || n_elements < 0 || n_elements > 16)
-    return handle_set_error(B200CHEM_EINVAL, "surrogate_gate: bad arguments");
-  if (ncells == 0) return 0;
-  if (!rhoY || !extF_rhoY || !T || !rhoH || !extF_rhoH || !pred || !ymean || !ystd || !accept ||
-      (n_elements > 0 && !elem))
-    return handle_set_error(B200CHEM_EINVAL, "surrogate_gate: null array");
-  GateParams P;
-  P.mech = *handle_mech(h);
-  P.rhoY = rhoY;
-  P.fY = extF_rhoY;
-  P.T = T;
-  P.rhoH = rhoH;
-  P.fH = extF_rhoH;
-  P.fct = fctCount;
-  P.ncells = ncells;
-  P.dt = dt;
-  P.pred = pred;
-  P.ymean = ymean;
-  P.ystd = ystd;
-  P.elem = elem;
-  P.ne = n_elements;
-  P.o = *opts;
-  P.accept = accept;
-  const cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int err;
-  switch (handle_species(h)) {
-    case 9: err = launch_gate<9>(P, st); break;
-    case 21: err = launch_gate<21>(P, st); break;
-    case 53: err = launch_gate<53>(P, st); break;
-    default: return handle_set_error(B200CHEM_EINVAL, "surrogate not compiled for this species count");
+// Features and every member's forward pass for cells c0 .. c0 + nc - 1.
+int predict_chunk(b200chem_surrogate* s, const double* rhoY, const double* T, long long ld, long long c0, long long nc,
+                  double dt, const InferBufs& B, long long rows, cudaStream_t st) {
+  FeatParams F{rhoY, T, ld, c0, nc, rows, log10(dt), s->xmean, s->xstd, B.x, s->terms};
+  int err = features_for(s->N, F, st);
+  if (err) return sur_err(err, "surrogate features: launch failed");
+  handle_count_launch(s->h);
+  const int split = s->terms == 2 ? (B200CHEM_GEMM_SPLIT_A | B200CHEM_GEMM_SPLIT_OUT) : 0;
+  const int split_a = s->terms == 2 ? B200CHEM_GEMM_SPLIT_A : 0;
+  const long long hw = (long long)s->terms * kHidden;
+  for (int mb = 0; mb < s->members; ++mb) {
+    const void* const* Wm = &s->W[mb * 4];
+    const float* const* bm = &s->b[mb * 4];
+    const __nv_bfloat16* a = B.x;
+    long long lda = (long long)s->terms * s->kin;
+    int K = s->kin;
+    __nv_bfloat16* outs[2] = {B.h0, B.h1};
+    for (int li = 0; li < 3; ++li) {
+      __nv_bfloat16* o = outs[li & 1];
+      if (b200chem_mlp_gemm_bf16(a, lda, Wm[li], K, (int)rows, kHidden, K, o, hw, bm[li], nullptr, 2 | split, 0,
+                                 B.err, st) != 0)
+        return sur_err(B200CHEM_ECUDA, "surrogate forward: hidden-layer GEMM rejected");
+      handle_count_launch(s->h);
+      a = o;
+      lda = hw;
+      K = kHidden;
+    }
+    float* pm = B.pred + (long long)mb * rows * s->kout;
+    if (b200chem_mlp_gemm_bf16(a, lda, Wm[3], kHidden, (int)rows, s->kout, kHidden, pm, s->kout, bm[3], nullptr,
+                               0 | split_a, s->nout, B.err, st) != 0)
+      return sur_err(B200CHEM_ECUDA, "surrogate forward: output GEMM rejected");
+    handle_count_launch(s->h);
   }
-  if (err) return handle_set_error(err, "surrogate_gate: launch failed");
+  return 0;
+}
+
+// Reads a little-endian value from the weights file.
+template <class T>
+T rd(const unsigned char* p) {
+  T v;
+  memcpy(&v, p, sizeof(T));
+  return v;
+}
+
+}  // namespace
+
+extern "C" b200chem_surrogate_handle b200chem_surrogate_load(b200chem_handle h, const void* data, size_t nbytes) {
+  if (!h || !data || nbytes < 256) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: bad arguments");
+    return nullptr;
+  }
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  if (memcmp(p, kMagic, 8) != 0) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: not a surrogate weights file (bad magic)");
+    return nullptr;
+  }
+  const uint32_t version = rd<uint32_t>(p + 8), hbytes = rd<uint32_t>(p + 12);
+  if (version != kFileVersion || hbytes < 128 || hbytes > nbytes) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: unsupported file version or header size");
+    return nullptr;
+  }
+  if (rd<uint64_t>(p + 16) != handle_digest(h)) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: the weights were trained for another mechanism (digest mismatch)");
+    return nullptr;
+  }
+  int32_t iv[12];
+  memcpy(iv, p + 24, sizeof(iv));
+  const int N = iv[0], nin = iv[1], nout = iv[2], hidden = iv[3], kin = iv[4], kout = iv[5], members = iv[6],
+            terms = iv[7], dtype = iv[8], min_members = iv[9], ne = iv[10];
+  if (N != handle_species(h) || nin != N + 2 || nout != N + 1 || hidden != kHidden || kin != sg_in(N) ||
+      kout != sg_out(N) || members < 1 || members > kMaxMembers || (terms != 1 && terms != 2) || dtype != 1 ||
+      ne < 0 || ne > kMaxElem) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: unsupported dimensions, member count, terms or dtype");
+    return nullptr;
+  }
+  double dv[7];
+  memcpy(dv, p + 72, sizeof(dv));
+  // body: xmean, xstd [nin] f32; ymean, ystd [nout] f32; tscale [nout] f64;
+  // elem [ne][N] f64; per member: W0 [256][kin] bf16, b0 [256] f32, W1, b1,
+  // W2, b2 ([256][256] bf16, [256] f32), W3 [kout][256] bf16, b3 [kout] f32
+  const size_t tsc_b = 8 * (size_t)nout, elem_b = 8 * (size_t)ne * N;
+  const size_t wsz[4] = {(size_t)kHidden * kin * 2, (size_t)kHidden * kHidden * 2, (size_t)kHidden * kHidden * 2,
+                         (size_t)kout * kHidden * 2};
+  const size_t bsz[4] = {(size_t)kHidden * 4, (size_t)kHidden * 4, (size_t)kHidden * 4, (size_t)kout * 4};
+  size_t member_b = 0;
+  for (int li = 0; li < 4; ++li) member_b += wsz[li] + bsz[li];
+  const size_t body = 4 * (2 * (size_t)nin + 2 * (size_t)nout) + tsc_b + elem_b + members * member_b;
+  if (hbytes + body != nbytes) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load: file size does not match its header");
+    return nullptr;
+  }
+  // device copy: every array 256-byte aligned
+  std::vector<size_t> sizes = {4 * (size_t)nin, 4 * (size_t)nin, 4 * (size_t)nout, 4 * (size_t)nout, tsc_b, elem_b};
+  for (int mb = 0; mb < members; ++mb)
+    for (int li = 0; li < 4; ++li) {
+      sizes.push_back(wsz[li]);
+      sizes.push_back(bsz[li]);
+    }
+  size_t total = 0;
+  for (size_t sz : sizes) total += align256(sz > 0 ? sz : 8);
+  std::vector<unsigned char> host(total, 0);
+  std::vector<size_t> offs;
+  size_t src = hbytes, dst = 0;
+  for (size_t sz : sizes) {
+    memcpy(host.data() + dst, p + src, sz);
+    offs.push_back(dst);
+    src += sz;
+    dst += align256(sz > 0 ? sz : 8);
+  }
+  auto* s = new b200chem_surrogate;
+  s->h = h;
+  s->device = handle_device(h);
+  s->N = N;
+  s->nin = nin;
+  s->nout = nout;
+  s->kin = kin;
+  s->kout = kout;
+  s->members = members;
+  s->terms = terms;
+  s->ne = ne;
+  s->opts.t_rel = dv[0];
+  s->opts.spread = dv[1];
+  s->opts.dT_cap = dv[2];
+  s->opts.gap = dv[3];
+  s->opts.tol_elem = dv[4];
+  s->opts.tol_mass = dv[5];
+  s->opts.resid = dv[6];
+  s->opts.min_members = min_members;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != s->device || cudaMalloc(&s->d_params, total) != cudaSuccess ||
+      cudaMemcpy(s->d_params, host.data(), total, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMallocHost(&s->h_count, 2 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    sur_err(B200CHEM_ECUDA, "surrogate_load: device upload failed (is the reactor's device current?)");
+    if (s->d_params) cudaFree(s->d_params);
+    delete s;
+    return nullptr;
+  }
+  unsigned char* base = static_cast<unsigned char*>(s->d_params);
+  s->xmean = reinterpret_cast<const float*>(base + offs[0]);
+  s->xstd = reinterpret_cast<const float*>(base + offs[1]);
+  s->ymean = reinterpret_cast<const float*>(base + offs[2]);
+  s->ystd = reinterpret_cast<const float*>(base + offs[3]);
+  s->tscale = reinterpret_cast<const double*>(base + offs[4]);
+  s->elem = reinterpret_cast<const double*>(base + offs[5]);
+  for (int mb = 0; mb < members; ++mb)
+    for (int li = 0; li < 4; ++li) {
+      s->W.push_back(base + offs[6 + (mb * 4 + li) * 2]);
+      s->b.push_back(reinterpret_cast<const float*>(base + offs[6 + (mb * 4 + li) * 2 + 1]));
+    }
+  return s;
+}
+
+extern "C" b200chem_surrogate_handle b200chem_surrogate_load_file(b200chem_handle h, const char* path) {
+  if (!h || !path) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load_file: bad arguments");
+    return nullptr;
+  }
+  FILE* f = fopen(path, "rb");
+  if (!f) {
+    sur_err(B200CHEM_EINVAL, "surrogate_load_file: cannot open the weights file");
+    return nullptr;
+  }
+  std::vector<unsigned char> buf;
+  unsigned char tmp[1 << 16];
+  size_t got;
+  while ((got = fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+  fclose(f);
+  return b200chem_surrogate_load(h, buf.data(), buf.size());
+}
+
+extern "C" int b200chem_surrogate_get_opts(b200chem_surrogate_handle s, b200chem_hybrid_opts* o) {
+  if (!s || !o) return sur_err(B200CHEM_EINVAL, "surrogate_get_opts: bad arguments");
+  *o = s->opts;
+  return 0;
+}
+
+extern "C" int b200chem_surrogate_destroy(b200chem_surrogate_handle s) {
+  if (!s) return 0;
+  if (s->last_stream) cudaStreamSynchronize(s->last_stream);
+  if (s->d_params) cudaFree(s->d_params);
+  if (s->d_scratch) cudaFree(s->d_scratch);
+  if (s->d_hy) cudaFree(s->d_hy);
+  if (s->h_count) cudaFreeHost(s->h_count);
+  delete s;
+  return 0;
+}
+
+extern "C" int b200chem_surrogate_infer(b200chem_surrogate_handle s, const double* rhoY, const double* T,
+                                        int64_t ncells, double dt, double* dy_mean, double* dT_spread, void* stream) {
+  if (!s || ncells < 0 || !(dt > 0.0)) return sur_err(B200CHEM_EINVAL, "surrogate_infer: bad arguments");
+  if (ncells == 0) return 0;
+  if (!rhoY || !T || !dy_mean) return sur_err(B200CHEM_EINVAL, "surrogate_infer: null array");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  s->last_stream = st;
+  const long long chunk = ncells < kChunkRows ? ((ncells + 127) / 128 * 128) : kChunkRows;
+  InferBufs B;
+  int err = ensure_infer(s, chunk, st, &B);
+  if (err) return err;
+  SCK(cudaMemsetAsync(B.err, 0, sizeof(int), st));
+  for (long long c0 = 0; c0 < ncells; c0 += chunk) {
+    const long long nc = std::min<long long>(chunk, ncells - c0);
+    const long long rows = (nc + 127) / 128 * 128;
+    err = predict_chunk(s, rhoY, T, ncells, c0, nc, dt, B, rows, st);
+    if (err) return err;
+    DecodeParams D{B.pred, rows, c0, nc, s->members, s->nout, s->kout, s->ymean, s->ystd, s->tscale, dy_mean,
+                   dT_spread};
+    const long long blocks = (nc + 127) / 128;
+    hy_decode<<<(unsigned)(blocks < 65535 ? blocks : 65535), 128, 0, st>>>(D);
+    SCK(cudaGetLastError());
+    handle_count_launch(s->h);
+  }
+  SCK(cudaMemcpyAsync(s->h_count + 1, B.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCK(cudaStreamSynchronize(st));
+  if (s->h_count[1]) return sur_err(B200CHEM_ECUDA, "surrogate_infer: a tensor-core completion wait timed out");
+  return 0;
+}
+
+extern "C" int b200chem_react_hybrid(b200chem_handle h, b200chem_surrogate_handle s, const b200chem_hybrid_opts* opts,
+                                     double* rhoY, const double* extF_rhoY, double* T, double* rhoH,
+                                     const double* extF_rhoH, double* fctCount, const int32_t* mask, int64_t ncells,
+                                     double* dt_react, double* time, void* stream, int32_t* cell_status,
+                                     b200chem_stats* stats, b200chem_hybrid_stats* hstats) {
+  if (!h || !s || s->h != h || ncells < 0 || !dt_react || !(*dt_react > 0.0))
+    return sur_err(B200CHEM_EINVAL, "react_hybrid: bad arguments (the surrogate must be loaded for this reactor)");
+  if (ncells > 0 && (!rhoY || !extF_rhoY || !T || !rhoH || !extF_rhoH))
+    return sur_err(B200CHEM_EINVAL, "react_hybrid: null state array");
+  if (ncells > 0x7fffffffLL) return sur_err(B200CHEM_ETOOBIG, "react_hybrid: ncells above 2^31-1");
+  const b200chem_hybrid_opts o = opts ? *opts : s->opts;
+  if (!(o.t_rel > 0.0) || o.spread < 0.0 || o.dT_cap < 0.0 || o.gap < 0.0 || o.tol_elem < 0.0 || o.tol_mass < 0.0 ||
+      o.resid < 0.0)
+    return sur_err(B200CHEM_EINVAL, "react_hybrid: bad acceptance options");
+  if (s->members < std::max(1, (int)o.min_members))
+    return sur_err(B200CHEM_EINVAL, "react_hybrid: fewer ensemble members than the options require");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  s->last_stream = st;
+  const double dt = *dt_react;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (hstats) memset(hstats, 0, sizeof(*hstats));
+  if (ncells == 0) {
+    if (time) *time += dt;
+    return 0;
+  }
+  const long long chunk = ncells < kChunkRows ? ((ncells + 127) / 128 * 128) : kChunkRows;
+  InferBufs B;
+  int err = ensure_infer(s, chunk, st, &B);
+  if (err) return err;
+  // hybrid scratch: reason counters and the reject count (256 B), the reject
+  // list, the compact state of the rejected cells, their status
+  const int N = s->N;
+  const long long cap = ncells;
+  const size_t list_b = align256(4 * (size_t)cap), state_b = align256(8 * (size_t)cap * (2 * N + 4));
+  const size_t need = 256 + list_b + state_b + align256(4 * (size_t)cap);
+  if (need > s->hy_bytes) {
+    if (s->d_hy) {
+      SCK(cudaStreamSynchronize(st));
+      cudaFree(s->d_hy);
+      s->d_hy = nullptr;
+      s->hy_bytes = 0;
+    }
+    if (cudaMalloc(&s->d_hy, need) != cudaSuccess) {
+      cudaGetLastError();
+      return sur_err(B200CHEM_ENOMEM, "react_hybrid: cannot allocate the fallback scratch");
+    }
+    s->hy_bytes = need;
+  }
+  unsigned char* q = static_cast<unsigned char*>(s->d_hy);
+  unsigned long long* reasons = reinterpret_cast<unsigned long long*>(q);
+  int* rej_count = reinterpret_cast<int*>(q + 8 * kReasons);
+  int* rej_list = reinterpret_cast<int*>(q + 256);
+  double* cY = reinterpret_cast<double*>(q + 256 + list_b);
+  double* cfY = cY + (size_t)N * cap;
+  double* cT = cfY + (size_t)N * cap;
+  double* cH = cT + cap;
+  double* cfH = cH + cap;
+  double* cfct = cfH + cap;
+  int* cstatus = reinterpret_cast<int*>(q + 256 + list_b + state_b);
+  SCK(cudaMemsetAsync(q, 0, 256, st));
+  SCK(cudaMemsetAsync(B.err, 0, sizeof(int), st));
+  GateParams G;
+  G.mech = *handle_mech(h);
+  G.rhoY = rhoY;
+  G.fY = extF_rhoY;
+  G.T = T;
+  G.rhoH = rhoH;
+  G.fH = extF_rhoH;
+  G.fct = fctCount;
+  G.mask = mask;
+  G.status = cell_status;
+  G.ld = ncells;
+  G.dt = dt;
+  G.pred = B.pred;
+  G.members = s->members;
+  G.ymean = s->ymean;
+  G.ystd = s->ystd;
+  G.tscale = s->tscale;
+  G.elem = s->elem;
+  G.ne = s->ne;
+  G.o = o;
+  G.rej_list = rej_list;
+  G.rej_count = rej_count;
+  G.reasons = reasons;
+  for (long long c0 = 0; c0 < ncells; c0 += chunk) {
+    const long long nc = std::min<long long>(chunk, ncells - c0);
+    const long long rows = (nc + 127) / 128 * 128;
+    err = predict_chunk(s, rhoY, T, ncells, c0, nc, dt, B, rows, st);
+    if (err) return err;
+    G.c0 = c0;
+    G.nc = nc;
+    G.rows = rows;
+    err = gate_for(N, G, handle_sm_count(h), st);
+    if (err) return sur_err(err, "react_hybrid: gate launch failed");
+    handle_count_launch(h);
+  }
+  // the rejected count sizes the fallback call
+  unsigned long long rs[kReasons];
+  SCK(cudaMemcpyAsync(s->h_count, rej_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCK(cudaMemcpyAsync(s->h_count + 1, B.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SCK(cudaMemcpyAsync(rs, reasons, sizeof(rs), cudaMemcpyDeviceToHost, st));
+  SCK(cudaStreamSynchronize(st));
+  if (s->h_count[1]) return sur_err(B200CHEM_ECUDA, "react_hybrid: a tensor-core completion wait timed out");
+  const long long nrej = s->h_count[0];
+  int rc = 0;
+  if (nrej > 0) {
+    MoveParams M{rej_list, rej_count, N, ncells, nrej, rhoY, T, rhoH, fctCount, extF_rhoY, extF_rhoH,
+                 cell_status, cY, cT, cH, cfY, cfH, cfct, cstatus};
+    const long long blocks = std::min<long long>((nrej + 255) / 256, 8LL * handle_sm_count(h));
+    hy_gather<<<(unsigned)blocks, 256, 0, st>>>(M);
+    SCK(cudaGetLastError());
+    handle_count_launch(h);
+    double dtr = dt;
+    rc = b200chem_react_flat(h, cY, cfY, cT, cH, cfH, cfct, nullptr, nrej, &dtr, nullptr, stream,
+                             cell_status ? cstatus : nullptr, stats);
+    if (rc != 0 && rc != B200CHEM_EINTEGRATE) return rc;
+    hy_scatter<<<(unsigned)blocks, 256, 0, st>>>(M, o.resid > 0.0 ? 2.0 : 0.0);
+    SCK(cudaGetLastError());
+    handle_count_launch(h);
+  }
+  long long predicted = 0;
+  for (int r = 0; r < kReasons; ++r) predicted += (long long)rs[r];
+  if (stats) {
+    stats->n_cells += (long long)rs[kAccept];
+    stats->n_masked += ncells - predicted;
+    SCK(cudaStreamSynchronize(st));  // synchronous, like react_flat with stats
+  }
+  if (hstats) {
+    hstats->predicted = predicted;
+    hstats->accepted = (long long)rs[kAccept];
+    hstats->rejected_spread = (long long)rs[kRejSpread];
+    hstats->rejected_cap = (long long)rs[kRejCap];
+    hstats->rejected_mass = (long long)rs[kRejMass];
+    hstats->rejected_elements = (long long)rs[kRejElem];
+    hstats->rejected_energy = (long long)rs[kRejEnergy];
+    hstats->rejected_negative = (long long)rs[kRejNegative];
+    hstats->rejected_residual = (long long)rs[kRejResid];
+    hstats->rejected_nonfinite = (long long)rs[kRejNonfinite];
+  }
+  if (time) *time += dt;
+  return rc;
+}
+
+extern "C" int b200chem_surrogate_features(b200chem_handle h, const double* rhoY, const double* T, int64_t ncells,
+                                           int64_t nrows, double dt, const float* xmean, const float* xstd,
+                                           int32_t terms, void* x_bf16, void* stream) {
+  if (!h || ncells < 0 || nrows < ncells || nrows % 128 || !(dt > 0.0) || !xmean || !xstd || !x_bf16 ||
+      (terms != 1 && terms != 2))
+    return handle_set_error(B200CHEM_EINVAL, "surrogate_features: bad arguments");
+  if (ncells > 0 && (!rhoY || !T)) return handle_set_error(B200CHEM_EINVAL, "surrogate_features: null state");
+  FeatParams P{rhoY, T, ncells, 0, ncells, nrows, log10(dt), xmean, xstd, static_cast<__nv_bfloat16*>(x_bf16),
+               terms};
+  const int err = features_for(handle_species(h), P, static_cast<cudaStream_t>(stream));
+  if (err == B200CHEM_EINVAL) return handle_set_error(err, "surrogate not compiled for this species count");
+  if (err) return handle_set_error(err, "surrogate_features: launch failed");
   handle_count_launch(h);
   return 0;
 }

@@ -270,13 +270,19 @@ class ReactorB200:
             self._h, views, len(items), dtp, tp, st, sp, stp), dt_react, time, stream, status, stats,
             raise_on_failure)
 
-    def advance_chemistry(self, items, dt, stream=None, status=None, stats=False, raise_on_failure=True):
+    def advance_chemistry(self, items, dt, stream=None, status=None, stats=False, raise_on_failure=True,
+                          skip_react=None):
         """PeleLM::advanceChemistry's box body (Source/PeleLMeX_Reactions.cpp:31-175) for a
         list of boxes, MKS fabs: each item is (box, rhoY_old, rhoH_old, T_old, rhoY_new,
         rhoH_new, T_new, extF_rhoY, extF_rhoH, fctCount, mask, I_R[, fab_lo]); fctCount,
-        mask and I_R may be None.  Returns stats (dict) when asked, else None."""
+        mask and I_R may be None.  skip_react (one flag per box, optional) marks the
+        covered boxes of advanceChemistryBAChem (m_baChemFlag == 0, :260-289): converted
+        and given I_R, but not reacted (fctCount = 0).  Returns stats (dict) when asked,
+        else None."""
         self._need()
         boxes = (_lib.ChemBox * max(len(items), 1))()
+        if skip_react is not None and len(skip_react) != len(items):
+            raise ValueError("skip_react needs one flag per box")
         for b, it in enumerate(items):
             box = it[0]
             flo = it[12] if len(it) > 12 and it[12] is not None else box.lo
@@ -287,6 +293,7 @@ class ReactorB200:
                      "fctCount", "mask", "I_R")
             for name, t in zip(names, it[1:12]):
                 setattr(x, name, array4(t, flo))
+            x.skip_react = 1 if (skip_react is not None and skip_react[b]) else 0
             if it[1].shape[0] != self.N or it[4].shape[0] != self.N:
                 raise ValueError(f"rhoY has {it[1].shape[0]} components, mechanism has {self.N}")
         st_obj = _lib.Stats()
@@ -298,6 +305,28 @@ class ReactorB200:
             raise ReactorError(f"advance_chemistry failed ({code}): {_lib.load().b200chem_last_error().decode()}",
                                status=status, stats=s)
         return s
+
+    def react_force(self, items, dt, stream=None):
+        """PeleLM::getScalarReactForce (Source/PeleLMeX_Reactions.cpp:437-475) for a list
+        of boxes, MKS fabs: each item is (box, rhoY_old, rhoH_old, rhoY_new, rhoH_new, I_R,
+        extF_rhoY, extF_rhoH[, fab_lo]); the two forcing fabs are written."""
+        self._need()
+        boxes = (_lib.ForceBox * max(len(items), 1))()
+        names = ("rhoY_old", "rhoH_old", "rhoY_new", "rhoH_new", "I_R", "extF_rhoY", "extF_rhoH")
+        for b, it in enumerate(items):
+            box = it[0]
+            flo = it[8] if len(it) > 8 and it[8] is not None else box.lo
+            x = boxes[b]
+            x.lo[:] = list(box.lo)
+            x.hi[:] = list(box.hi)
+            for name, t in zip(names, it[1:8]):
+                if t is None:
+                    raise ValueError(f"react_force: {name} is required")
+                setattr(x, name, array4(t, flo))
+            for k in (1, 3, 5, 6):
+                if it[k].shape[0] != self.N:
+                    raise ValueError(f"{names[k - 1]} has {it[k].shape[0]} components, mechanism has {self.N}")
+        _lib.check(_lib.load().b200chem_react_force(self._h, boxes, len(items), float(dt), _stream_ptr(stream)))
 
     def react_flat(self, rhoY, extF_rhoY, T, rhoH, extF_rhoH, fctCount=None, mask=None, dt_react=1e-6,
                    time=0.0, stream=None, status=None, stats=False, raise_on_failure=True):

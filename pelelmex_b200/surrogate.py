@@ -1,28 +1,46 @@
 """Learned surrogate of the HP reaction advance and the hybrid reactor.
 
-The surrogate is an MLP that predicts the state change over dt_react:
+The surrogate is an ensemble of MLPs that predict the state change over
+dt_react:
 
     x = (T, log10(Y_k + 1e-20) for k < N, log10 dt)          N + 2 inputs
     x -> 256 -> 256 -> 256 (GELU) -> (dT, dY_k)              N + 1 outputs
 
-inputs and outputs standardised by training-set statistics, BF16 weights and
-activations with FP32 accumulation.  Every matrix product of inference and
-training runs on the tensor cores through the library's hand-written tcgen05
-GEMM (b200chem_mlp_gemm_bf16) with fused bias / GELU / GELU-backward
-epilogues; the network input and the acceptance gate are library kernels too
-(b200chem_surrogate_features, b200chem_surrogate_gate).  PyTorch holds the
-device buffers and does the transposes, reductions and the Adam update.
+Inputs are standardised by training-set statistics.  Outputs are
+u_j = asinh(dy_j / s_j) (s_T = 0.02 K, s_k a tenth of the median |dY_k| of the
+training pairs), standardised: the transform gives every decade of change the
+same resolution, so a 0.5 K and a 50 K temperature change are learnt to the
+same relative accuracy.
 
-It is trained on (state, dt) -> state pairs labelled by the plain GPU BDF of
-the same reactor.  The hybrid reactor predicts every cell, accepts a
-prediction only when the gate's conservation, energy and one-step residual
-checks pass, and integrates the rejected cells with the BDF.
+Precision: BF16 weights, FP32 accumulation on the tensor cores (the
+library's hand-written tcgen05 GEMM, b200chem_mlp_gemm_bf16).  Inputs and
+hidden activations travel as two BF16 terms (hi = bf16(v), lo = bf16(v - hi),
+about 16 significant bits): a single BF16 term resolves T only to ~2 K and
+log10 Y to ~0.01, which alone moves the predicted dT of flame cells by several
+times the 1e-4 relative bar.  Both terms are multiplied by the same weights
+and summed in the FP32 accumulator.
+
+Training runs on the GPU through the same GEMMs (forward, dz = (dz W) *
+gelu'(pre), dW = dz^T a) and a fused Adam kernel (b200chem_mlp_adam); PyTorch
+holds the buffers and does the transposes and bias-gradient sums.  Training
+pairs are (state, dt) -> state labelled by the plain GPU BDF of the same
+reactor.
+
+The hybrid reactor (b200chem_react_hybrid) predicts every cell with every
+member, accepts a prediction only when the ensemble agrees within a fraction
+of the temperature bar, the change is within the range where the ensemble's
+agreement bounds its error, the raw prediction conserves mass and elements,
+T from (h, Y) agrees with the predicted T, and a one-step implicit residual
+holds; accepted cells get the element- and energy-consistent state, the
+others are integrated by the BDF, all in one library call.
 """
 from __future__ import annotations
 
 import ctypes
 import math
-from dataclasses import dataclass
+import struct
+from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 
@@ -31,6 +49,13 @@ from . import mechanism as mechmod
 
 HIDDEN = 256
 EPI_F32, EPI_BF16, EPI_GELU, EPI_DGELU = 0, 1, 2, 3
+SPLIT_OUT, SPLIT_A = 0x10, 0x20
+T_SCALE = 0.02  # K: asinh scale of the temperature change
+Y_SCALE_FLOOR = 1e-9  # smallest asinh scale of a mass-fraction change
+
+MAGIC = b"B2CHSURR"
+FILE_VERSION = 1
+HEADER_BYTES = 256
 
 
 def _torch():
@@ -51,45 +76,44 @@ class GemmError(RuntimeError):
 
 
 def gemm(A, B, C, bias=None, epi=EPI_F32, aux=None, n_valid=0, err=None):
-    """C = epi(A . B^T + bias) on the tensor cores (see b200chem_mlp_gemm_bf16)."""
-    M, K = A.shape
-    N = B.shape[0]
+    """C = epi(A . B^T + bias) on the tensor cores (b200chem_mlp_gemm_bf16);
+    K is B's row length (A holds two terms of it when SPLIT_A is set)."""
+    M = A.shape[0]
+    N, K = B.shape
     code = _lib.load().b200chem_mlp_gemm_bf16(
         A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), M, N, K, C.data_ptr(), C.stride(0),
         bias.data_ptr() if bias is not None else None, aux.data_ptr() if aux is not None else None, epi, n_valid,
         err.data_ptr() if err is not None else None, _stream())
     if code != 0:
-        raise GemmError(f"tensor-core GEMM rejected M={M} N={N} K={K} epi={epi} (code {code})")
+        raise GemmError(f"tensor-core GEMM rejected M={M} N={N} K={K} epi={epi:#x} (code {code})")
     return C
 
 
 @dataclass
-class GateOpts:
-    """Acceptance thresholds (b200chem_gate_opts).  The defaults keep the
-    accepted cells of the drm19-shaped flame field within 1e-4 relative T of
-    the BDF with margin (held-out seeded cells, two-member ensemble): raw mass
-    and element errors below 1e-3 (then corrected exactly), T from (h, Y)
-    within 0.05 K of the predicted T, predicted |dT| <= 0.2 K, and the
-    one-step implicit residual of the temperature within 10 % of its change."""
-    rtol: float = 1e-6
-    atol: float = 0.0
-    tol_T: float = 0.05
-    tol_elem: float = 1e-3
-    tol_mass: float = 1e-3
-    rchange: float = 0.1
-    dT_max: float = 0.2
-    t_source: int = 1
-    residual_t_only: int = 1
+class HybridOpts:
+    """Acceptance rule of the hybrid reactor (b200chem_hybrid_opts).  All
+    temperature bounds are in units of t_rel * T (the error bar itself)."""
+    t_rel: float = 1e-4     # relative T error the accepted cells are held to
+    spread: float = 0.05    # max deviation of a member's dT from the ensemble mean
+    dT_cap: float = 10.0    # max |predicted dT| (the ensemble's shared bias grows with the change)
+    gap: float = 5.0        # max |T(h, Y_pred) - T_pred| before the energy projection
+    tol_elem: float = 2e-3  # raw element-conservation error, relative to the atom content
+    tol_mass: float = 2e-3  # raw mass-conservation error, relative
+    resid: float = 0.0      # one-step residual bound (0: off)
+    min_members: int = 2
 
     def ctypes(self):
-        return _lib.GateOpts(self.rtol, self.atol, self.tol_T, self.tol_elem, self.tol_mass, self.rchange,
-                             self.dT_max, self.t_source, self.residual_t_only)
+        return _lib.HybridOpts(self.t_rel, self.spread, self.dT_cap, self.gap, self.tol_elem, self.tol_mass,
+                               self.resid, self.min_members, 0)
+
+    def as_tuple(self):
+        return (self.t_rel, self.spread, self.dT_cap, self.gap, self.tol_elem, self.tol_mass, self.resid)
 
 
 class MLPSurrogate:
-    """The network, its normalisation, and its tensor-core training."""
+    """One network of the ensemble and its tensor-core training."""
 
-    def __init__(self, mech, seed: int = 0, device="cuda:0"):
+    def __init__(self, mech, seed: int = 0, device="cuda:0", terms: int = 2):
         torch = _torch()
         if isinstance(mech, str):
             mech = mechmod.builtin(mech)
@@ -97,6 +121,7 @@ class MLPSurrogate:
         self.N = mech.n_species
         self.nin, self.nout = self.N + 2, self.N + 1
         self.kin, self.kout = _pad16(self.nin), _pad16(self.nout)
+        self.terms = terms
         self.device = torch.device(device)
         g = torch.Generator(device="cpu").manual_seed(seed)
         dims = [(HIDDEN, self.kin, self.nin), (HIDDEN, HIDDEN, HIDDEN), (HIDDEN, HIDDEN, HIDDEN),
@@ -113,7 +138,9 @@ class MLPSurrogate:
         self.xstd = torch.ones(self.nin, device=self.device)
         self.ymean = torch.zeros(self.nout, device=self.device)
         self.ystd = torch.ones(self.nout, device=self.device)
+        self.tscale = torch.ones(self.nout, dtype=torch.float64, device=self.device)
         self._adam = None
+        self._err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._sync_bf16()
 
     # ------------------------------------------------------------ weights
@@ -122,62 +149,83 @@ class MLPSurrogate:
         self.Wb = [W.to(torch.bfloat16).contiguous() for W in self.W]
         self.WbT = [W.t().contiguous() for W in self.Wb]
 
+    def share_normalisation(self, other: "MLPSurrogate"):
+        self.xmean, self.xstd, self.ymean, self.ystd, self.tscale = (other.xmean, other.xstd, other.ymean,
+                                                                     other.ystd, other.tscale)
+
     def state_dict(self):
         return {"W": [W.cpu() for W in self.W], "b": [b.cpu() for b in self.b], "xmean": self.xmean.cpu(),
-                "xstd": self.xstd.cpu(), "ymean": self.ymean.cpu(), "ystd": self.ystd.cpu(), "N": self.N}
+                "xstd": self.xstd.cpu(), "ymean": self.ymean.cpu(), "ystd": self.ystd.cpu(),
+                "tscale": self.tscale.cpu(), "N": self.N, "terms": self.terms}
 
     def load_state_dict(self, d):
-        self.W = [W.to(self.device) for W in d["W"]]
-        self.b = [b.to(self.device) for b in d["b"]]
+        self.W = [W.to(self.device).float() for W in d["W"]]
+        self.b = [b.to(self.device).float() for b in d["b"]]
         for k in ("xmean", "xstd", "ymean", "ystd"):
-            setattr(self, k, d[k].to(self.device))
+            setattr(self, k, d[k].to(self.device).float())
+        self.tscale = d["tscale"].to(self.device).double()
+        self.terms = int(d.get("terms", self.terms))
+        self._adam = None
         self._sync_bf16()
 
     # ----------------------------------------------------------- features
     def raw_features(self, rhoY, T, dt):
-        """Unstandardised inputs [ncells, N + 2] (FP32, for statistics)."""
+        """Unstandardised inputs [ncells, N + 2] (FP64, for statistics)."""
         torch = _torch()
         Y = rhoY / rhoY.sum(dim=0, keepdim=True)
         lg = torch.log10(Y.clamp_min(0.0) + 1e-20)
         dtc = torch.full_like(T, math.log10(dt))
-        return torch.cat([T[None], lg, dtc[None]]).t().float()
+        return torch.cat([T[None], lg, dtc[None]]).t()
 
     def features(self, reactor, rhoY, T, dt, nrows):
-        """Standardised BF16 network input [nrows, kin] (library kernel)."""
+        """Standardised BF16 network input [nrows, terms * kin] (library kernel)."""
         torch = _torch()
-        x = torch.empty((nrows, self.kin), dtype=torch.bfloat16, device=self.device)
+        x = torch.empty((nrows, self.terms * self.kin), dtype=torch.bfloat16, device=self.device)
         _lib.check(_lib.load().b200chem_surrogate_features(
             reactor._h, rhoY.data_ptr(), T.data_ptr(), T.shape[0], nrows, float(dt), self.xmean.data_ptr(),
-            self.xstd.data_ptr(), x.data_ptr(), _stream()))
+            self.xstd.data_ptr(), self.terms, x.data_ptr(), _stream()))
         return x
 
     # ------------------------------------------------------------ forward
     def forward(self, x, train=False):
-        """x: [B, kin] BF16 (B % 128 == 0) -> standardised outputs [B, kout] FP32."""
+        """x: [B, terms * kin] BF16 (B % 128 == 0) -> standardised outputs [B, kout] FP32."""
         torch = _torch()
         B = x.shape[0]
-        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        split = SPLIT_A if self.terms == 2 else 0
+        out_split = SPLIT_OUT if self.terms == 2 else 0
         acts, pres = [x], []
         h = x
         for li in range(3):
             pre = torch.empty((B, HIDDEN), dtype=torch.float32, device=self.device) if train else None
-            out = torch.empty((B, HIDDEN), dtype=torch.bfloat16, device=self.device)
-            gemm(h, self.Wb[li], out, self.b[li], EPI_GELU, aux=pre, err=err)
+            out = torch.empty((B, self.terms * HIDDEN), dtype=torch.bfloat16, device=self.device)
+            gemm(h, self.Wb[li], out, self.b[li], EPI_GELU | split | out_split, aux=pre, err=self._err)
             acts.append(out)
             pres.append(pre)
             h = out
         y = torch.zeros((B, self.kout), dtype=torch.float32, device=self.device)
-        gemm(h, self.Wb[3], y, self.b[3], EPI_F32, n_valid=self.nout, err=err)
-        self._err = err
+        gemm(h, self.Wb[3], y, self.b[3], EPI_F32 | split, n_valid=self.nout, err=self._err)
         return (y, (acts, pres)) if train else y
 
     def check_error(self):
         if int(self._err.item()) != 0:
             raise GemmError("a tensor-core completion wait timed out")
 
+    def decode(self, y):
+        """Standardised outputs -> physical changes (dT, dY_k) [B, N + 1], FP64."""
+        torch = _torch()
+        u = y[:, :self.nout].double() * self.ystd.double() + self.ymean.double()
+        return torch.sinh(u) * self.tscale
+
+    def encode(self, dy):
+        """Physical changes [B, N + 1] -> standardised targets (FP32)."""
+        torch = _torch()
+        u = torch.asinh(dy / self.tscale)
+        return ((u - self.ymean.double()) / self.ystd.double()).float()
+
     # ----------------------------------------------------------- backward
     def loss_and_grads(self, x, target, weights):
-        """Weighted MSE on standardised outputs; gradients by the tensor cores."""
+        """Weighted MSE on standardised outputs; gradients by the tensor cores.
+        The weight gradients use the high term of each two-term activation."""
         torch = _torch()
         B = x.shape[0]
         y, (acts, pres) = self.forward(x, train=True)
@@ -187,7 +235,6 @@ class MLPSurrogate:
         d[:, :self.nout] = 2.0 * diff / B
         db = [None] * 4
         dW = [None] * 4
-        err = self._err
         dz = d.to(torch.bfloat16)
         for li in range(3, -1, -1):
             db[li] = dz.float().sum(dim=0)
@@ -196,51 +243,41 @@ class MLPSurrogate:
             mpad = (out_f + 127) // 128 * 128
             dzT = torch.zeros((mpad, B), dtype=torch.bfloat16, device=self.device)
             dzT[:out_f] = dz.t()
-            aT = acts[li].t().contiguous()
-            Cw = torch.empty((mpad, aT.shape[0]), dtype=torch.float32, device=self.device)
-            gemm(dzT, aT, Cw, err=err)
-            dW[li] = Cw[:out_f]
+            width = self.W[li].shape[1]
+            aT = acts[li][:, :width].t().contiguous()
+            Cw = torch.empty((mpad, width), dtype=torch.float32, device=self.device)
+            gemm(dzT, aT, Cw, err=self._err)
+            dW[li] = Cw[:out_f].contiguous()
             if li > 0:
                 # dz_prev = (dz W) * gelu'(pre_prev)
                 nxt = torch.empty((B, HIDDEN), dtype=torch.bfloat16, device=self.device)
-                gemm(dz, self.WbT[li], nxt, None, EPI_DGELU, aux=pres[li - 1], err=err)
+                gemm(dz, self.WbT[li], nxt, None, EPI_DGELU, aux=pres[li - 1], err=self._err)
                 dz = nxt
         return loss, dW, db
 
     def adam_step(self, dW, db, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        """One fused Adam step (b200chem_mlp_adam) per tensor; refreshes the BF16 copies."""
         torch = _torch()
         if self._adam is None:
             self._adam = {"t": 0, "m": [torch.zeros_like(p) for p in self.W + self.b],
                           "v": [torch.zeros_like(p) for p in self.W + self.b]}
         st = self._adam
         st["t"] += 1
-        c1 = 1 - beta1 ** st["t"]
-        c2 = 1 - beta2 ** st["t"]
-        params = self.W + self.b
-        grads = list(dW) + list(db)
-        for p, g, m, v in zip(params, grads, st["m"], st["v"]):
-            m.mul_(beta1).add_(g, alpha=1 - beta1)
-            v.mul_(beta2).addcmul_(g, g, value=1 - beta2)
-            p.addcdiv_(m / c1, (v / c2).sqrt_().add_(eps), value=-lr)
-        # keep the padding exactly zero
-        self.W[0][:, self.nin:] = 0
-        self.W[3][self.nout:] = 0
-        self.b[3][self.nout:] = 0
-        self._sync_bf16()
+        L = _lib.load()
+        for i, (p, g) in enumerate(zip(self.W + self.b, list(dW) + list(db))):
+            rows, cols = (p.shape[0], p.shape[1]) if p.dim() == 2 else (1, p.shape[0])
+            wb = self.Wb[i].data_ptr() if i < 4 else None
+            wbt = self.WbT[i].data_ptr() if i < 4 else None
+            code = L.b200chem_mlp_adam(p.data_ptr(), g.contiguous().data_ptr(), st["m"][i].data_ptr(),
+                                       st["v"][i].data_ptr(), rows, cols, float(lr), beta1, beta2, eps, st["t"],
+                                       wb, wbt, _stream())
+            if code != 0:
+                raise GemmError(f"adam step rejected (code {code})")
 
     # ----------------------------------------------------------- training
-    def fit_normalisation(self, raw_x, dy):
-        torch = _torch()
-        self.xmean = raw_x.mean(dim=0)
-        self.xstd = raw_x.std(dim=0).clamp_min(1e-3)
-        self.ymean = dy.mean(dim=0)
-        floor = torch.full_like(self.ymean, 1e-12)
-        floor[0] = 1e-6
-        self.ystd = torch.maximum(dy.std(dim=0), floor)
-
     def train(self, x_all, y_all, steps=4000, batch=8192, lr=2e-3, lr_end=2e-5, weights=None, log_every=0,
               seed=0):
-        """x_all [S, kin] BF16 standardised inputs; y_all [S, nout] FP32 standardised targets."""
+        """x_all [S, terms * kin] BF16 standardised inputs; y_all [S, nout] FP32 standardised targets."""
         torch = _torch()
         S = x_all.shape[0]
         if weights is None:
@@ -258,9 +295,6 @@ class MLPSurrogate:
         self.check_error()
         return hist
 
-    def standardise_targets(self, dy):
-        return (dy - self.ymean) / self.ystd
-
 
 def element_matrix(mech):
     return np.ascontiguousarray(mech.element_matrix(), dtype=np.float64)
@@ -268,108 +302,238 @@ def element_matrix(mech):
 
 def label_pairs(reactor, field, device="cuda:0"):
     """Inputs and BDF-labelled changes for every cell of a field: returns
-    (rhoY0, T0, dy) with dy [ncells, N + 1] = (T1 - T0, Y1 - Y0)."""
+    (rhoY0, T0, dy, fct) with dy [ncells, N + 1] = (T1 - T0, Y1 - Y0) in FP64
+    and fct the BDF's right-hand-side count per cell."""
     torch = _torch()
-    rhoY = torch.tensor(field.rhoY, device=device)
-    T = torch.tensor(field.T, device=device)
-    rhoH = torch.tensor(field.rhoH, device=device)
+    rhoY = torch.as_tensor(field.rhoY, device=device)
+    T = torch.as_tensor(field.T, device=device)
+    rhoH = torch.as_tensor(field.rhoH, device=device)
     fY = torch.zeros_like(rhoY)
     fH = torch.zeros_like(T)
     rY1, T1, rH1 = rhoY.clone(), T.clone(), rhoH.clone()
-    reactor.react_flat(rY1, fY, T1, rH1, fH, dt_react=field.dt)
+    fct = torch.zeros_like(T)
+    reactor.react_flat(rY1, fY, T1, rH1, fH, fct, dt_react=field.dt)
     Y0 = rhoY / rhoY.sum(dim=0, keepdim=True)
     Y1 = rY1 / rY1.sum(dim=0, keepdim=True)
-    dy = torch.cat([(T1 - T)[None], Y1 - Y0]).t().contiguous().float()
-    return rhoY, T, dy
+    dy = torch.cat([(T1 - T)[None], Y1 - Y0]).t().contiguous()
+    return rhoY, T, dy, fct
+
+
+class Ensemble:
+    """Networks sharing one normalisation, with the acceptance rule they were
+    calibrated for; saved in the library's versioned weights format."""
+
+    def __init__(self, members, opts: HybridOpts | None = None):
+        self.members = list(members)
+        self.s = self.members[0]
+        self.opts = opts or HybridOpts()
+
+    @property
+    def mech(self):
+        return self.s.mech
+
+    def predict(self, reactor, rhoY, T, dt):
+        """Decoded predictions of every member, [M, ncells, N + 1] FP64."""
+        torch = _torch()
+        nc = T.shape[0]
+        nrows = (nc + 127) // 128 * 128
+        x = self.s.features(reactor, rhoY, T, dt, nrows)
+        return torch.stack([m.decode(m.forward(x)[:nc]) for m in self.members])
+
+    # --------------------------------------------------------- file format
+    def to_bytes(self) -> bytes:
+        """The versioned weights file (layout documented in include/b200chem.h,
+        b200chem_surrogate_load)."""
+        s = self.s
+        flat = mechmod.flatten(s.mech)
+        from . import mechgen
+        digest = mechgen.mechanism_digest(flat)
+        o = self.opts
+        hdr = MAGIC + struct.pack("<II", FILE_VERSION, HEADER_BYTES) + struct.pack("<Q", digest)
+        elem = element_matrix(s.mech)
+        hdr += struct.pack("<12i", s.N, s.nin, s.nout, HIDDEN, s.kin, s.kout, len(self.members), s.terms, 1,
+                           int(o.min_members), elem.shape[0], 0)
+        hdr += struct.pack("<7d", *o.as_tuple())
+        hdr += b"\0" * (HEADER_BYTES - len(hdr))
+        assert len(hdr) == HEADER_BYTES
+        body = b"".join(np.ascontiguousarray(t.detach().cpu().numpy(), dtype=np.float32).tobytes()
+                        for t in (s.xmean, s.xstd, s.ymean, s.ystd))
+        body += np.ascontiguousarray(s.tscale.cpu().numpy(), dtype=np.float64).tobytes()
+        body += elem.tobytes()
+        for m in self.members:
+            for li in range(4):
+                body += m.Wb[li].contiguous().cpu().view(_torch().int16).numpy().tobytes()
+                body += np.ascontiguousarray(m.b[li].cpu().numpy(), dtype=np.float32).tobytes()
+        return hdr + body
+
+    def save(self, path):
+        Path(path).write_bytes(self.to_bytes())
+
+    @classmethod
+    def from_bytes(cls, data: bytes, mech, device="cuda:0") -> "Ensemble":
+        torch = _torch()
+        if data[:8] != MAGIC:
+            raise ValueError("not a surrogate weights file (bad magic)")
+        version, hbytes = struct.unpack_from("<II", data, 8)
+        if version != FILE_VERSION:
+            raise ValueError(f"surrogate weights file version {version}, expected {FILE_VERSION}")
+        (digest,) = struct.unpack_from("<Q", data, 16)
+        N, nin, nout, hidden, kin, kout, M, terms, dtype, min_members, ne, _ = struct.unpack_from("<12i", data, 24)
+        opts = struct.unpack_from("<7d", data, 72)
+        if isinstance(mech, str):
+            mech = mechmod.builtin(mech)
+        from . import mechgen
+        if mechgen.mechanism_digest(mechmod.flatten(mech)) != digest:
+            raise ValueError("surrogate weights were trained for a different mechanism (digest mismatch)")
+        if hidden != HIDDEN or N != mech.n_species or dtype != 1:
+            raise ValueError("surrogate weights file has unsupported dimensions or dtype")
+        off = hbytes
+
+        def take(n, dt):
+            nonlocal off
+            a = np.frombuffer(data, dtype=dt, count=n, offset=off).copy()
+            off += n * np.dtype(dt).itemsize
+            return a
+        norm = [torch.tensor(take(n, np.float32), device=device) for n in (nin, nin, nout, nout)]
+        tscale = torch.tensor(take(nout, np.float64), device=device)
+        take(ne * N, np.float64)  # element matrix: the library's gate reads it; here it follows from mech
+        members = []
+        dims = [(hidden, kin), (hidden, hidden), (hidden, hidden), (kout, hidden)]
+        for _ in range(M):
+            m = MLPSurrogate(mech, device=device, terms=terms)
+            for li, (r, c) in enumerate(dims):
+                w = torch.from_numpy(take(r * c, np.int16).reshape(r, c)).view(torch.bfloat16)
+                m.W[li] = w.float().to(device)
+                m.b[li] = torch.tensor(take(r, np.float32), device=device)
+            m.xmean, m.xstd, m.ymean, m.ystd = norm
+            m.tscale = tscale
+            m._sync_bf16()
+            members.append(m)
+        if off != len(data):
+            raise ValueError("surrogate weights file has trailing or missing bytes")
+        return cls(members, HybridOpts(*opts, min_members=min_members))
+
+    @classmethod
+    def load(cls, path, mech, device="cuda:0") -> "Ensemble":
+        return cls.from_bytes(Path(path).read_bytes(), mech, device)
+
+
+def fit_normalisation(s: MLPSurrogate, raw_x, dy):
+    """Input statistics, asinh scales and output statistics from training pairs."""
+    torch = _torch()
+    s.xmean = raw_x.mean(dim=0).float()
+    s.xstd = raw_x.std(dim=0).clamp_min(1e-3).float()
+    n = dy.shape[0]
+    sub = dy[torch.randperm(n, device=dy.device)[:min(n, 500_000)]]
+    # species: a tenth of the median change, floored at 1e-9 -- changes of Y
+    # below that are at the BDF's own absolute tolerance (atol 1e-12 on
+    # rho Y, rho ~ 1e-3 g/cm^3) and carry no temperature information
+    sY = (sub[:, 1:].abs().median(dim=0).values * 0.1).clamp_min(Y_SCALE_FLOOR)
+    s.tscale = torch.cat([torch.tensor([T_SCALE], dtype=torch.float64, device=dy.device), sY])
+    u = torch.asinh(dy / s.tscale)
+    s.ymean = u.mean(dim=0).float()
+    s.ystd = u.std(dim=0).float().clamp_min(1e-6)
+
+
+def train_ensemble(reactor, mech, fields, members=4, steps=8000, batch=16384, lr=2e-3, seed=0, t_weight=None,
+                   bag=0.8, terms=2, log=None):
+    """Label every cell of `fields` with the BDF, fit one normalisation and
+    train `members` networks, each on its own random share `bag` of the pairs
+    (different initialisations and batch orders)."""
+    torch = _torch()
+    raws, dys, xs_src = [], [], []
+    s0 = MLPSurrogate(mech, seed=seed, terms=terms)
+    for f in fields:
+        rY, T, dy, _ = label_pairs(reactor, f)
+        raws.append(s0.raw_features(rY, T, f.dt))
+        dys.append(dy)
+        xs_src.append((rY, T, f.dt))
+    dy = torch.cat(dys)
+    fit_normalisation(s0, torch.cat(raws), dy)
+    del raws
+    xs = []
+    for rY, T, dt in xs_src:
+        nc = T.shape[0]
+        xs.append(s0.features(reactor, rY, T, dt, (nc + 127) // 128 * 128)[:nc])
+    del xs_src
+    x = torch.cat(xs)
+    y = s0.encode(dy)
+    del xs, dy
+    w = torch.ones(s0.nout, device=s0.device)
+    w[0] = float(t_weight if t_weight is not None else s0.N)
+    S = x.shape[0]
+    nets = []
+    for mbr in range(members):
+        s = s0 if mbr == 0 else MLPSurrogate(mech, seed=seed + mbr, terms=terms)
+        s.share_normalisation(s0)
+        if bag < 1.0:
+            gen = torch.Generator(device=s.device).manual_seed(1000 + seed + mbr)
+            sub = torch.randperm(S, device=s.device, generator=gen)[: int(bag * S)]
+            xm, ym = x[sub], y[sub]
+        else:
+            xm, ym = x, y
+        hist = s.train(xm, ym, steps=steps, batch=batch, lr=lr, weights=w, seed=seed + 7 * mbr,
+                       log_every=max(1, steps // 4))
+        if log:
+            log(f"member {mbr}: loss {[round(h[1], 5) for h in hist]}")
+        nets.append(s)
+        del xm, ym
+    return nets
 
 
 class HybridReactor:
-    """Surrogate-first reaction advance with gated fallback to the BDF.
+    """Surrogate-first reaction advance with gated fallback to the BDF: one
+    library call (b200chem_react_hybrid) per react."""
 
-    `surrogate` is one network or a list of networks sharing one
-    normalisation (an ensemble): with several, the gate sees their mean
-    prediction and a cell whose members disagree on dT by more than
-    tol_ensemble (K) is rejected before the conservation / energy / residual
-    checks."""
-
-    def __init__(self, reactor, surrogate, gate: GateOpts | None = None, tol_ensemble: float = 0.05):
-        torch = _torch()
+    def __init__(self, reactor, ensemble: Ensemble, opts: HybridOpts | None = None):
         self.r = reactor
-        self.members = list(surrogate) if isinstance(surrogate, (list, tuple)) else [surrogate]
-        self.s = self.members[0]
-        self.gate = gate or GateOpts()
-        self.tol_ensemble = tol_ensemble
-        self.elem = torch.tensor(element_matrix(self.s.mech), device=self.s.device)
+        self.ens = ensemble
+        self.opts = opts or ensemble.opts
+        self._sur = None
         self.last = {}
 
-    def react_flat(self, rhoY, extF_rhoY, T, rhoH, extF_rhoH, fctCount=None, dt_react=1e-6):
-        torch = _torch()
-        nc = T.shape[0]
-        if nc == 0:
-            return 0
-        nrows = (nc + 127) // 128 * 128
-        x = self.s.features(self.r, rhoY, T, dt_react, nrows)
-        pred = self.s.forward(x)
-        if len(self.members) > 1:
-            preds = [pred] + [m.forward(x) for m in self.members[1:]]
-            pred = torch.stack(preds).mean(dim=0)
-            spread = torch.stack([(p[:, 0] - pred[:, 0]).abs() for p in preds]).amax(dim=0) * self.s.ystd[0]
-            pred[spread > self.tol_ensemble, 0] = float("nan")  # the gate rejects a non-finite dT
-        accept = torch.empty(nc, dtype=torch.int32, device=T.device)
-        go = self.gate.ctypes()
-        _lib.check(_lib.load().b200chem_surrogate_gate(
-            self.r._h, rhoY.data_ptr(), extF_rhoY.data_ptr(), T.data_ptr(), rhoH.data_ptr(), extF_rhoH.data_ptr(),
-            fctCount.data_ptr() if fctCount is not None else None, nc, float(dt_react), pred.data_ptr(),
-            self.s.ymean.data_ptr(), self.s.ystd.data_ptr(), self.elem.data_ptr(), self.elem.shape[0],
-            ctypes.byref(go), accept.data_ptr(), _stream()))
-        rej = torch.nonzero(accept != 1).flatten()
-        nrej = int(rej.numel())
-        if nrej:
-            rY = rhoY.index_select(1, rej).contiguous()
-            fY = extF_rhoY.index_select(1, rej).contiguous()
-            Tr = T.index_select(0, rej).contiguous()
-            rH = rhoH.index_select(0, rej).contiguous()
-            fH = extF_rhoH.index_select(0, rej).contiguous()
-            fc = torch.zeros(nrej, dtype=torch.float64, device=T.device)
-            self.r.react_flat(rY, fY, Tr, rH, fH, fc, dt_react=dt_react)
-            rhoY.index_copy_(1, rej, rY)
-            T.index_copy_(0, rej, Tr)
-            rhoH.index_copy_(0, rej, rH)
-            if fctCount is not None:
-                fctCount.index_copy_(0, rej, fc + 2.0)
-        counts = torch.bincount((-accept).clamp_min(0), minlength=6).tolist()
-        self.last = {"cells": nc, "rejected": nrej, "accepted_fraction": 1.0 - nrej / nc, "accepted": accept == 1,
-                     "rejected_by": {"mass": counts[1], "elements": counts[2], "energy": counts[3],
-                                     "residual": counts[4], "change": counts[5]}}
-        return nrej
+    def _handle(self):
+        if self._sur is None:
+            blob = self.ens.to_bytes()
+            buf = ctypes.create_string_buffer(blob, len(blob))
+            L = _lib.load()
+            h = L.b200chem_surrogate_load(self.r._h, buf, len(blob))
+            if not h:
+                raise _lib.B200ChemError(-1, L.b200chem_last_error().decode())
+            self._sur = h
+        return self._sur
 
+    def close(self):
+        if self._sur is not None:
+            _lib.load().b200chem_surrogate_destroy(self._sur)
+            self._sur = None
 
-def train_ensemble(reactor, mech, fields, members=2, steps=4000, batch=8192, lr=2e-3, seed=0):
-    """Label every cell of `fields` with the BDF, fit one normalisation and
-    train `members` networks (different initialisations and batch orders)."""
-    torch = _torch()
-    rhoYs, Ts, dys, dts = [], [], [], []
-    for f in fields:
-        rY, T, dy = label_pairs(reactor, f)
-        rhoYs.append(rY)
-        Ts.append(T)
-        dys.append(dy)
-        dts.append(f.dt)
-    nets = []
-    s0 = MLPSurrogate(mech, seed=seed)
-    raw = torch.cat([s0.raw_features(rY, T, dt) for rY, T, dt in zip(rhoYs, Ts, dts)])
-    dy = torch.cat(dys)
-    s0.fit_normalisation(raw, dy)
-    xs = []
-    for rY, T, dt in zip(rhoYs, Ts, dts):
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def react_flat(self, rhoY, extF_rhoY, T, rhoH, extF_rhoH, fctCount=None, mask=None, dt_react=1e-6,
+                   time=0.0, stream=None, status=None, stats=True, raise_on_failure=True):
+        from .reactor import ReactorError, _stream_ptr
+        sur = self._handle()
         nc = T.shape[0]
-        xs.append(s0.features(reactor, rY, T, dt, (nc + 127) // 128 * 128)[:nc])
-    x = torch.cat(xs)
-    y = s0.standardise_targets(dy)
-    for mbr in range(members):
-        s = s0 if mbr == 0 else MLPSurrogate(mech, seed=seed + mbr)
-        if mbr:
-            s.xmean, s.xstd, s.ymean, s.ystd = s0.xmean, s0.xstd, s0.ymean, s0.ystd
-        s.train(x, y, steps=steps, batch=batch, lr=lr, seed=seed + 7 * mbr)
-        nets.append(s)
-    return nets
+        dtp = ctypes.c_double(dt_react)
+        tp = ctypes.c_double(time)
+        st = _lib.Stats()
+        hs = _lib.HybridStats()
+        o = self.opts.ctypes()
+        code = _lib.load().b200chem_react_hybrid(
+            self.r._h, sur, ctypes.byref(o), rhoY.data_ptr(), extF_rhoY.data_ptr(), T.data_ptr(), rhoH.data_ptr(),
+            extF_rhoH.data_ptr(), fctCount.data_ptr() if fctCount is not None else None,
+            mask.data_ptr() if mask is not None else None, nc, ctypes.byref(dtp), ctypes.byref(tp),
+            _stream_ptr(stream), status.data_ptr() if status is not None else None,
+            ctypes.byref(st) if stats else None, ctypes.byref(hs) if stats else None)
+        if code != 0 and (code != -4 or raise_on_failure):
+            raise ReactorError(f"hybrid react failed ({code}): {_lib.load().b200chem_last_error().decode()}")
+        if stats:
+            h = hs.as_dict()
+            self.last = dict(h, cells=nc, accepted_fraction=h["accepted"] / max(1, h["predicted"]),
+                             stats=st.as_dict())
+        return dtp.value, tp.value

@@ -1,40 +1,144 @@
-"""Train the surrogate ensemble on BDF-labelled cells of seeded flame fields.
+"""Train, calibrate and save the surrogate ensemble of the hybrid reactor.
 
-    python -m pelelmex_b200.train_surrogate [--cells 1048576] [--steps 4000] [--out FILE]
+    python -m pelelmex_b200.train_surrogate --out pelelmex_b200/surrogates/synth_ch4_21.b2s
 
-The training fields are seeded random samples of the drm19-shaped 128^3
-flame field with seeds distinct from the evaluation fields; every cell is
-labelled by the plain GPU BDF at rtol 1e-8 / atol 1e-12.
+1. Training fields: the drm19-shaped 128^3 flame field (workloads.flame_ch4)
+   for seeds 10..15, generated on the host cores (a process pool started
+   before the first GPU call).  Every cell is labelled at dt_react 1e-6 s and
+   1e-5 s by the plain GPU BDF at rtol 1e-8 / atol 1e-12: 2 x 6 x 2,097,152
+   (state, dt) -> state pairs.
+2. Training: `members` networks on the tensor cores (surrogate.train_ensemble),
+   each on its own random 80 % of the pairs.
+3. Calibration of the acceptance rule on a held-out field (seed 5, never
+   trained on): for each candidate rule, b200chem_react_hybrid reacts the
+   field at both time steps and the largest temperature error of an accepted
+   cell against the plain BDF is measured; the most permissive rule whose
+   worst accepted cell stays within `margin` of the 1e-4 bar at both time
+   steps is kept (the candidates are ordered from strict to permissive).
+4. The versioned weights file (the format of b200chem_surrogate_load) carries
+   the networks, their normalisation, the element matrix and the rule.
 """
 from __future__ import annotations
 
 import argparse
+import json
+import multiprocessing as mp
+import os
 import time
+from types import SimpleNamespace
+
+import numpy as np
+
+EDGE = 128
+
+# candidate acceptance rules, strict to permissive: (spread, dT_cap, gap) in bars
+CANDIDATES = [(0.03, 5.0, 2.0), (0.05, 5.0, 3.0), (0.05, 10.0, 3.0), (0.08, 10.0, 3.0), (0.1, 10.0, 3.0),
+              (0.1, 15.0, 3.0), (0.12, 15.0, 3.0), (0.15, 15.0, 3.0), (0.15, 20.0, 3.0), (0.2, 20.0, 5.0)]
+
+
+def _gen(a):
+    from pelelmex_b200 import mechanism as M, workloads as W
+    name, seed, lo, hi = a
+    f = W.flame_ch4(M.builtin(name), seed=seed, cells=np.arange(lo, hi, dtype=np.int64))
+    return f.rhoY, f.T, f.rhoH
+
+
+def flame_fields(pool, name, seeds, edge=EDGE, chunks=64):
+    """Full flame fields (rhoY, T, rhoH) of the given seeds, generated in parallel."""
+    n = edge ** 3
+    step = (n + chunks - 1) // chunks
+    out = {}
+    for s in seeds:
+        parts = pool.map(_gen, [(name, s, lo, min(n, lo + step)) for lo in range(0, n, step)])
+        out[s] = (np.concatenate([p[0] for p in parts], axis=1), np.concatenate([p[1] for p in parts]),
+                  np.concatenate([p[2] for p in parts]))
+    return out
+
+
+def calibrate(reactor, ens, fields, dts, margin, log=print):
+    """Pick the most permissive candidate rule whose worst accepted cell stays
+    within `margin` bars at every dt on the held-out fields.  Returns the rule
+    and the per-candidate table."""
+    import torch
+    from .surrogate import HybridOpts, HybridReactor
+    dev = torch.device("cuda:0")
+    plain = {}
+    for key, (rY, T, rH) in fields.items():
+        for dt in dts:
+            a = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
+            fY, fH = torch.zeros_like(a[0]), torch.zeros_like(a[1])
+            fct = torch.zeros_like(a[1])
+            reactor.react_flat(a[0], fY, a[1], a[2], fH, fct, dt_react=dt)
+            plain[(key, dt)] = (a[1], fct)
+    table, best = [], None
+    for spread, cap, gap in CANDIDATES:
+        opts = HybridOpts(spread=spread, dT_cap=cap, gap=gap)
+        row = {"spread": spread, "dT_cap": cap, "gap": gap}
+        ok_all = True
+        for key, (rY, T, rH) in fields.items():
+            for dt in dts:
+                a = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
+                fY, fH = torch.zeros_like(a[0]), torch.zeros_like(a[1])
+                h = HybridReactor(reactor, ens, opts)
+                h.react_flat(a[0], fY, a[1], a[2], fH, None, dt_react=dt)
+                T_ref, fct = plain[(key, dt)]
+                err = ((a[1] - T_ref).abs() / (opts.t_rel * T_ref)).max().item()
+                acc = h.last["accepted"] / h.last["predicted"]
+                h.close()
+                row[f"{key}_dt{dt:g}"] = {"accepted": round(acc, 4), "max_err_bars": round(err, 4)}
+                ok_all &= err <= margin
+        row["within_margin"] = bool(ok_all)
+        table.append(row)
+        log(json.dumps(row))
+        if ok_all:
+            best = opts
+    return best, table
 
 
 def main():
-    import torch
-
-    from . import mechanism as M, workloads as W
-    from .reactor import ReactorB200
-    from .surrogate import train_ensemble
-
     p = argparse.ArgumentParser()
     p.add_argument("--mechanism", default="synth_ch4_21")
-    p.add_argument("--cells", type=int, default=1 << 20)
-    p.add_argument("--steps", type=int, default=4000)
-    p.add_argument("--members", type=int, default=2)
-    p.add_argument("--dt", type=float, default=1e-6)
-    p.add_argument("--seed", type=int, default=10)
-    p.add_argument("--out", default="surrogate_ensemble.pt")
+    p.add_argument("--out", required=True)
+    p.add_argument("--seeds", default="10,11,12,13,14,15", help="training field seeds")
+    p.add_argument("--val-seed", type=int, default=5, help="held-out calibration field seed")
+    p.add_argument("--members", type=int, default=8)
+    p.add_argument("--steps", type=int, default=12000)
+    p.add_argument("--batch", type=int, default=16384)
+    p.add_argument("--margin", type=float, default=0.5, help="worst accepted cell allowed, in bars")
+    p.add_argument("--report", default=None, help="JSON file for the calibration table")
     a = p.parse_args()
+    seeds = [int(s) for s in a.seeds.split(",")]
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+        fields = flame_fields(pool, a.mechanism, seeds + [a.val_seed])
+    print(f"fields generated in {time.time() - t0:.1f} s", flush=True)
+
+    import torch
+    from . import mechanism as M
+    from .reactor import ReactorB200
+    from .surrogate import Ensemble, train_ensemble
     mech = M.builtin(a.mechanism)
     r = ReactorB200(mech, rtol=1e-8, atol=1e-12, max_order=5).init()
-    t0 = time.time()
-    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, a.cells, seed=a.seed), dt=a.dt, seed=a.seed)
-    nets = train_ensemble(r, mech, [f], members=a.members, steps=a.steps)
-    torch.save([n.state_dict() for n in nets], a.out)
-    print(f"trained {len(nets)} networks on {a.cells} cells in {time.time() - t0:.1f} s -> {a.out}")
+    dts = (1e-6, 1e-5)
+    t1 = time.time()
+    train = [SimpleNamespace(rhoY=fields[s][0], T=fields[s][1], rhoH=fields[s][2], dt=dt) for s in seeds
+             for dt in dts]
+    nets = train_ensemble(r, mech, train, members=a.members, steps=a.steps, batch=a.batch,
+                          log=lambda m: print(m, f"({time.time() - t1:.0f} s)", flush=True))
+    torch.cuda.synchronize()
+    print(f"trained {a.members} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
+    ens = Ensemble(nets)
+    rule, table = calibrate(r, ens, {f"seed{a.val_seed}": fields[a.val_seed]}, dts, a.margin)
+    if rule is None:
+        raise SystemExit("no candidate acceptance rule keeps the held-out field within the margin")
+    ens.opts = rule
+    ens.save(a.out)
+    print(f"saved {a.out}: rule {rule}", flush=True)
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump({"rule": rule.__dict__, "table": table, "members": a.members, "steps": a.steps,
+                       "train_seeds": seeds, "val_seed": a.val_seed, "dts": dts}, f, indent=1)
+    r.close()
 
 
 if __name__ == "__main__":

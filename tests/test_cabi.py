@@ -26,7 +26,7 @@ def test_library_exports_all_declared_symbols():
     lib = ctypes.CDLL(str(build.build()))
     missing = [n for n in declared() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.b200chem_version() == 1
+    assert lib.b200chem_version() == 2
 
 
 def test_struct_layouts_match_header():
@@ -34,6 +34,15 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Array4) == 8 + 3 * 8 + 6 * 4
     assert ctypes.sizeof(_lib.BoxView) == 24 + 7 * ctypes.sizeof(_lib.Array4)
     assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 10 * 4  # two doubles and ten int32 fields
+    assert ctypes.sizeof(_lib.ChemBox) == 24 + 11 * ctypes.sizeof(_lib.Array4) + 8
+    assert ctypes.sizeof(_lib.ForceBox) == 24 + 7 * ctypes.sizeof(_lib.Array4)
+
+
+def test_null_arguments_of_the_box_list_calls_are_rejected_without_gpu():
+    from pelelmex_b200 import _lib
+    L = _lib.load()
+    assert L.b200chem_react_force(None, None, 0, 1e-6, None) == -1
+    assert L.b200chem_advance_chemistry(None, None, 0, 1e-6, None, None, None) == -1
 
 
 def test_null_handle_is_rejected_without_gpu():

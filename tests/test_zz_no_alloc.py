@@ -109,3 +109,34 @@ def test_noalloc_rejects_oversized_scratch():
         assert "scratch" in L.b200chem_last_error().decode()
     finally:
         r.close()
+
+
+@pytest.mark.parametrize("kernel", ["thread", "rounds"])
+def test_noalloc_rejects_other_integrators(kernel):
+    # only the group integrator has an allocation-free form; a handle built for
+    # another integrator is refused rather than silently run on the group one
+    L = _lib.load()
+    noalloc_fn = _fn(L, "b200chem_react_flat_noalloc")
+    mech = M.builtin("synth_h2_9")
+    f = W.premixed_h2(mech, edge=4)
+    r = ReactorB200("synth_h2_9", rtol=1e-8, atol=1e-12, max_order=5, kernel=kernel).init(2, f.ncells)
+    try:
+        with pytest.raises(AssertionError, match="group integrator only"):
+            _steps(noalloc_fn, r, f, nsteps=1)
+    finally:
+        r.close()
+
+
+def test_noalloc_counts_its_launches():
+    L = _lib.load()
+    noalloc_fn = _fn(L, "b200chem_react_flat_noalloc")
+    mech = M.builtin("synth_h2_9")
+    f = W.premixed_h2(mech, edge=4)
+    r = ReactorB200("synth_h2_9", rtol=1e-8, atol=1e-12, max_order=5, kernel="group").init(2, f.ncells)
+    try:
+        n0 = r.kernel_launches()
+        _steps(noalloc_fn, r, f, nsteps=1)
+        # the box-descriptor store and the integrator
+        assert r.kernel_launches() - n0 == 2
+    finally:
+        r.close()
