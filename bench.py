@@ -63,8 +63,6 @@ def parse():
     p.add_argument("--no-hybrid", action="store_true", help="plain BDF only (no surrogate arm)")
     p.add_argument("--no-autotune", action="store_true", help="default launch shape (no autotuner pass)")
     p.add_argument("--tune-cells", type=int, default=262144, help="cells of the autotuner's sample")
-    p.add_argument("--train-cells", type=int, default=524288, help="BDF-labelled training cells of the surrogate")
-    p.add_argument("--train-steps", type=int, default=3000, help="optimizer steps per ensemble member")
     return p.parse_args()
 
 
@@ -80,9 +78,13 @@ def workload_config(args):
     return {"workload": f"flame_ch4 {args.edge}^3{sub} drm19-shaped (synth_ch4_21: 21 species + T, 84 reactions), "
                         f"dt_react {args.dt:g} s, P 1 atm",
             "mechanism": MECH, "cells": args.cells or args.edge ** 3, "dt_react": args.dt, "rtol": RTOL, "atol": ATOL,
-            "max_order": QMAX,
-            "integrator": "plain GPU BDF, round-based (FP64 state/rates, FP32 Newton inverse + FP64 refinement)",
-            "l2": "inputs 750 MB > L2, state restored from a device copy between steps"}
+            "max_order": QMAX, "l2": "inputs 750 MB > L2, state restored from a device copy between steps"}
+
+
+GPU_INTEGRATOR = "plain GPU BDF, round-based (FP64 state/rates, FP32 Newton inverse + FP64 refinement)"
+HYBRID_INTEGRATOR = "hybrid: surrogate ensemble (tcgen05 BF16 MLPs) with gated fallback to the plain GPU BDF"
+CPU_INTEGRATOR = ("CPU oracle: FP64 C restatement of the dense-direct variable-order BDF (CVODE denseAJ_direct "
+                  "algorithm), OpenMP over cells")
 
 
 # ------------------------------------------------------------------ clocks
@@ -146,12 +148,37 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- utilities
-def load_field(args):
+def _gen_chunk(a):
     from pelelmex_b200 import mechanism as mechmod, workloads
+    edge, seed, lo, hi = a
+    f = workloads.flame_ch4(mechmod.builtin(MECH), edge=edge, seed=seed, cells=np.arange(lo, hi, dtype=np.int64))
+    return f.rhoY, f.T, f.rhoH
+
+
+def flame_field(args, seed=2):
+    """The full flame field, generated by a pool of host processes (started
+    before any CUDA call; each cell depends only on its index and the seed, so
+    the chunks concatenate to exactly workloads.flame_ch4's field)."""
+    import multiprocessing as mp
+    from types import SimpleNamespace
+    n = args.edge ** 3
+    chunks = 64
+    step = (n + chunks - 1) // chunks
+    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+        parts = pool.map(_gen_chunk, [(args.edge, seed, lo, min(n, lo + step)) for lo in range(0, n, step)])
+    rhoY = np.concatenate([p[0] for p in parts], axis=1)
+    T = np.concatenate([p[1] for p in parts])
+    rhoH = np.concatenate([p[2] for p in parts])
+    return SimpleNamespace(rhoY=rhoY, T=T, rhoH=rhoH, frhoY=np.zeros_like(rhoY), frhoH=np.zeros_like(T),
+                           dt=args.dt, ncells=n)
+
+
+def load_field(args):
+    from pelelmex_b200 import mechanism as mechmod
     mech = mechmod.builtin(MECH)
     if args.cells:
         return mech, sample_field(mech, args, args.cells, 4242)
-    return mech, workloads.flame_ch4(mech, edge=args.edge, dt=args.dt)
+    return mech, flame_field(args)
 
 
 def fp64_peak_tflops(torch, dev):
@@ -160,12 +187,12 @@ def fp64_peak_tflops(torch, dev):
     a = torch.randn(n, n, dtype=torch.float64, device=dev)
     b = torch.randn(n, n, dtype=torch.float64, device=dev)
     for _ in range(2):
-        torch.matmul(a, b)
+        a @ b
     best = 1e30
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        torch.matmul(a, b)
+        a @ b
         e1.record()
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
@@ -174,35 +201,32 @@ def fp64_peak_tflops(torch, dev):
 
 
 def fp32_peak_tflops(torch, dev):
-    """Live FP32 (CUDA-core) reference peak: cuBLAS SGEMM 8192^3 without
-    TF32, best of 5."""
+    """Live FP32 reference peak: cuBLAS SGEMM 8192^3 without TF32, best of 5."""
     n = 8192
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
-    try:
-        a = torch.randn(n, n, dtype=torch.float32, device=dev)
-        b = torch.randn(n, n, dtype=torch.float32, device=dev)
-        for _ in range(2):
-            torch.matmul(a, b)
-        best = 1e30
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            torch.matmul(a, b)
-            e1.record()
-            torch.cuda.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        del a, b
-    finally:
-        torch.backends.cuda.matmul.allow_tf32 = prev
+    a = torch.randn(n, n, dtype=torch.float32, device=dev)
+    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        a @ b
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def sample_field(mech, args, n, seed):
+def sample_field(mech, args, n, seed, dt=None):
     """n seeded random cells of the full field, generated directly."""
     from pelelmex_b200 import workloads
     idx = workloads.sample_cells(args.edge ** 3, n, seed=seed)
-    return workloads.flame_ch4(mech, edge=args.edge, dt=args.dt, cells=idx)
+    return workloads.flame_ch4(mech, edge=args.edge, dt=dt or args.dt, cells=idx)
 
 
 def cpu_sample_run(mech, args, seconds: float, nthreads: int = 0):
@@ -225,30 +249,38 @@ def cpu_sample_run(mech, args, seconds: float, nthreads: int = 0):
         n = min(total, int(n * min(8.0, max(1.5, 0.6 * seconds / max(el, 1e-3)))))
 
 
-def sample_accuracy(mech, field, rY_dev, T_dev, n=2048):
-    """Max errors of the GPU result on n seeded cells: against the oracle at
-    rtol 1e-8 / atol 1e-12 and against the oracle at rtol 1e-12 / atol 1e-20;
-    the oracle's own error against the tight solve beside them."""
+TIGHT = dict(rtol=1e-12, atol=1e-20)
+
+
+def sample_accuracy(mech, args, dt, gpu, n=2048):
+    """Errors on n seeded cells of the field at dt: the GPU results given in
+    `gpu` ({name: (T [ncells], rhoY [N, ncells]) device tensors}) against the
+    CPU oracle at rtol 1e-8 / atol 1e-12 and against the oracle's tight FP64
+    solve (rtol 1e-12 / atol 1e-20); the oracle's own error beside them."""
+    import torch
     from oracle import oracle as orc
     from pelelmex_b200 import mechanism as mechmod, workloads
-    idx = workloads.sample_cells(field.ncells, min(n, field.ncells), seed=2468)
-    sub = field.subset(idx)
-    it = __import__("torch").as_tensor(idx, device=T_dev.device)
-    gT = T_dev.index_select(0, it).cpu().numpy()
-    gY = rY_dev.index_select(1, it).cpu().numpy()
+    idx = workloads.sample_cells(args.edge ** 3, n, seed=2468)
+    sub = workloads.flame_ch4(mech, edge=args.edge, dt=dt, cells=idx)
     o = orc.Oracle(mechmod.flatten(mech))
-    kw = dict(max_order=QMAX, max_steps=MAXSTEPS, nthreads=orc.max_threads())
-    ref = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=RTOL, atol=ATOL, **kw)
-    tight = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, sub.dt, rtol=1e-12, atol=1e-20, **kw)
+    kw = dict(max_order=QMAX, max_steps=100000, nthreads=orc.max_threads())
+    ref = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, dt, rtol=RTOL, atol=ATOL, **kw)
+    tight = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, dt, **TIGHT, **kw)
     rho = sub.rhoY.sum(axis=0)
 
     def err(T, Y, RT, RY):
         return {"max_rel_T": float(np.max(np.abs(T - RT) / RT)),
                 "max_abs_Y": float(np.max(np.abs(Y - RY).max(axis=0) / rho))}
-    return {"sample_cells": int(len(idx)), "gpu_vs_oracle": err(gT, gY, ref["T"], ref["rhoY"]),
-            "gpu_vs_tight": err(gT, gY, tight["T"], tight["rhoY"]),
-            "oracle_vs_tight": err(ref["T"], ref["rhoY"], tight["T"], tight["rhoY"]),
-            "tight": "oracle BDF at rtol 1e-12 / atol 1e-20", "tolerances": f"rtol {RTOL:g} / atol {ATOL:g}"}
+    out = {"sample_cells": int(len(idx)), "oracle_vs_oracle_tight": err(ref["T"], ref["rhoY"], tight["T"],
+                                                                        tight["rhoY"]),
+           "oracle_tight": "oracle BDF at rtol 1e-12 / atol 1e-20", "tolerances": f"rtol {RTOL:g} / atol {ATOL:g}"}
+    it = torch.as_tensor(idx, device=next(iter(gpu.values()))[0].device)
+    for name, (T, rY) in gpu.items():
+        gT = T.index_select(0, it).cpu().numpy()
+        gY = rY.index_select(1, it).cpu().numpy()
+        out[f"{name}_vs_oracle"] = err(gT, gY, ref["T"], ref["rhoY"])
+        out[f"{name}_vs_oracle_tight"] = err(gT, gY, tight["T"], tight["rhoY"])
+    return out
 
 
 def emit(line):
@@ -283,15 +315,41 @@ def run_reference(args, rank, world):
     emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_full, "higher_is_better": True,
           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+          "integrator": CPU_INTEGRATOR,
+          "extrapolated": {"ms_per_step": True, "sample_cells_per_step": n, "cells": total},
           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
 
 
 # ------------------------------------------------------------- B200 arm
-def run_b200(args, rank, world, local_rank):
+SURROGATE = ROOT / "pelelmex_b200" / "surrogates" / f"{MECH}.b2s"
+
+
+def time_steps(fn, restore, steps, warmup, stream, barrier):
+    """warmup untimed calls, then `steps` calls each bracketed by CUDA events
+    on the launching stream (state restored before every call, outside the
+    events).  Returns the per-step milliseconds."""
+    import torch
+    for _ in range(warmup):
+        restore()
+        fn()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for s in range(steps):
+        restore()
+        ev[s][0].record(stream)
+        fn()
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def run_b200(args, rank, world, local_rank, field):
     import torch
     import torch.distributed as dist
-    from pelelmex_b200 import perfmodel
+    from pelelmex_b200 import mechanism as mechmod, perfmodel
     from pelelmex_b200.reactor import ReactorB200
 
     dev = torch.device("cuda", local_rank)
@@ -299,7 +357,7 @@ def run_b200(args, rank, world, local_rank):
     props = torch.cuda.get_device_properties(dev)
     bus = getattr(props, "pci_bus_id", None)
     bus_id = f"{props.pci_domain_id:08x}:{bus:02x}:{props.pci_device_id:02x}.0" if bus is not None else None
-    mech, field = load_field(args)
+    mech = mechmod.builtin(MECH)
     nc = field.ncells
     N = mech.n_species
     cfg = workload_config(args)
@@ -319,121 +377,119 @@ def run_b200(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
-    # launch shape: the autotuner times react on a seeded sample of the same
-    # field distribution (untimed, before the warm-up)
-    if not args.no_autotune:
+    # launch shape: the cached one of this mechanism and GPU, else the
+    # autotuner on a seeded sample of the same field distribution (untimed,
+    # before the warm-up), then cached
+    cache = ROOT / "pelelmex_b200" / "tuning" / f"{MECH}.b2t"
+    if not args.no_autotune and r.load_tuning(cache):
+        launch_tuning = dict(r.get_tuning(), source=f"cache {cache.relative_to(ROOT)}")
+    elif not args.no_autotune:
         tf = sample_field(mech, args, min(args.tune_cells, nc), seed=77)
         td = {k: torch.tensor(getattr(tf, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
         t0 = time.perf_counter()
         tuning, tune_ms = r.autotune(td["rhoY"], td["frhoY"], td["T"], td["rhoH"], td["frhoH"], field.dt,
                                      max_trials=32)
-        cfg["launch_tuning"] = dict(tuning, sample_cells=tf.ncells, sample_ms=round(tune_ms, 3),
-                                    seconds=round(time.perf_counter() - t0, 2))
+        launch_tuning = dict(tuning, sample_cells=tf.ncells, sample_ms=round(tune_ms, 3),
+                             seconds=round(time.perf_counter() - t0, 2), source="autotuned")
         del td
+        if rank == 0:
+            cache.parent.mkdir(exist_ok=True)
+            r.save_tuning(cache)
     else:
-        cfg["launch_tuning"] = dict(r.get_tuning(), autotuned=False)
+        launch_tuning = dict(r.get_tuning(), autotuned=False)
 
-    # warm-up; the first call also collects the integrator's counters
-    counters = None
-    for w in range(args.warmup):
-        restore()
-        res = r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt, stats=(w == 0))
-        if w == 0:
-            counters = res[2]
+    def plain_step(dt):
+        return lambda: r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=dt)
+
+    # integrator counters of one call (untimed)
+    restore()
+    counters = r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt, stats=True)[2]
     torch.cuda.synchronize()
 
-    # timed region: K steps, each bracketed by events on the launching stream
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier()
-    torch.cuda.synchronize()
+    # headline timed region: K plain BDF steps at the configured dt
     launches0 = r.kernel_launches()
     with ClockSampler(bus_id) as clk:
-        for s in range(args.steps):
-            restore()
-            ev[s][0].record(stream)
-            r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
-            ev[s][1].record(stream)
-        torch.cuda.synchronize()
-    launches = r.kernel_launches() - launches0
-    barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    ms = sum(step_ms) / len(step_ms)
-    ms = sharding.step_time_max(ms, dev)
+        step_ms = time_steps(plain_step(field.dt), restore, args.steps, args.warmup, stream, barrier)
+    launches = (r.kernel_launches() - launches0) * args.steps // (args.steps + args.warmup)
+    ms = sharding.step_time_max(sum(step_ms) / len(step_ms), dev)
     value = world * nc / (ms * 1e-3)
     plain = {"value": value, "unit": UNIT, "ms_per_step": ms, "step_ms": step_ms}
 
-    # hybrid arm: surrogate ensemble (trained here, untimed) + gated BDF fallback
-    hybrid, h = None, None
-    if not args.no_hybrid:
-        from pelelmex_b200 import workloads
-        from pelelmex_b200.surrogate import HybridReactor, train_ensemble
+    # both time steps of the drm19 config: plain BDF, hybrid, accuracy against
+    # a tight FP64 solve of every cell
+    from pelelmex_b200.surrogate import Ensemble, HybridReactor
+    ens = Ensemble.load(SURROGATE, mech) if (SURROGATE.exists() and not args.no_hybrid) else None
+    rt = ReactorB200(MECH, rtol=TIGHT["rtol"], atol=TIGHT["atol"], max_order=QMAX, max_steps=100000,
+                     lu_fp64=True).init()
+    blocks = {}
+    other = 1e-5 if field.dt == 1e-6 else 1e-6
+    k2 = max(3, args.steps // 4)
+    hy_headline = None
+    for dt in (field.dt, other):
+        blk = {"dt_react": dt}
+        if dt == field.dt:
+            blk["plain_ms_per_step"] = ms
+        else:
+            pms = time_steps(plain_step(dt), restore, k2, 2, stream, barrier)
+            blk["plain_ms_per_step"] = sharding.step_time_max(sum(pms) / len(pms), dev)
+            blk["plain_steps"] = k2
+        blk["plain_value"] = world * nc / (blk["plain_ms_per_step"] * 1e-3)
+        # the plain result and the tight reference of every cell
         restore()
-        r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
-        ref_T, ref_rY = T.clone(), rY.clone()
-        tf = workloads.flame_ch4(mech, cells=workloads.sample_cells(args.edge ** 3, args.train_cells, seed=10),
-                                 dt=args.dt, seed=10)
+        r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=dt)
+        pT, pY = T.clone(), rY.clone()
+        restore()
         t0 = time.perf_counter()
-        nets = train_ensemble(r, mech, [tf], members=2, steps=args.train_steps)
+        rt.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], dt_react=dt)
         torch.cuda.synchronize()
-        train_s = time.perf_counter() - t0
-        h = HybridReactor(r, nets)
-        restore()
-        h.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
-        torch.cuda.synchronize()
-        terr = float(((T - ref_T).abs() / ref_T).max().item())
-        yerr = float(((rY - ref_rY).abs().max(dim=0).values / ref_rY.sum(dim=0)).max().item())
-        accepted = h.last["accepted_fraction"]
-        hev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(args.steps)]
-        barrier()
-        torch.cuda.synchronize()
-        hl0 = r.kernel_launches()
-        for s_ in range(args.steps):
+        tT, tY = T.clone(), rY.clone()
+        blk["tight_solve"] = {"what": "GPU BDF over every cell at rtol 1e-12 / atol 1e-20 with an FP64 Newton LU",
+                              "seconds": round(time.perf_counter() - t0, 2)}
+        rho = base["rhoY"].sum(dim=0)
+
+        def errs(Tx, Yx, Tr, Yr):
+            return {"max_rel_T": float(((Tx - Tr).abs() / Tr).max().item()),
+                    "max_abs_Y": float(((Yx - Yr).abs().max(dim=0).values / rho).max().item())}
+        blk["plain_vs_tight"] = errs(pT, pY, tT, tY)
+        gpu_res = {"plain": (pT, pY), "gpu_tight": (tT, tY)}
+        if ens is not None:
+            h = HybridReactor(r, ens)
+
+            def hstep(dt=dt, h=h):
+                return h.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=dt, stats=False)
             restore()
-            hev[s_][0].record(stream)
-            h.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
-            hev[s_][1].record(stream)
-        torch.cuda.synchronize()
-        hlaunch = r.kernel_launches() - hl0
-        barrier()
-        hstep = [a.elapsed_time(b) for a, b in hev]
-        hms = sum(hstep) / len(hstep)
-        hms = sharding.step_time_max(hms, dev)
-        # the tensor-core forward pass alone (4 GEMMs over every cell)
-        nrows = (nc + 127) // 128 * 128
-        x = nets[0].features(r, base["rhoY"], base["T"], field.dt, nrows)
-        for _ in range(2):
-            nets[0].forward(x)
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(5):
-            nets[0].forward(x)
-        f1.record(stream)
-        torch.cuda.synchronize()
-        mlp_ms = f0.elapsed_time(f1) / 5
-        s0 = nets[0]
-        mlp_flops = 2.0 * nrows * (s0.kin * 256 + 2 * 256 * 256 + 256 * s0.kout)
-        bf16_peak = None
-        mp = ROOT / "MEASURED_PEAKS.json"
-        if mp.exists():
-            try:
-                bf16_peak = json.loads(mp.read_text()).get("bf16_tflops")
-            except (ValueError, OSError):
-                bf16_peak = None
-        hybrid = {"value": world * nc / (hms * 1e-3), "unit": UNIT, "ms_per_step": hms, "step_ms": hstep,
-                  "speedup_vs_plain_gpu_bdf": ms / hms, "accepted_fraction": accepted,
-                  "rejected_by": h.last["rejected_by"], "max_rel_T_err_vs_plain_bdf": terr,
-                  "max_abs_Y_err_vs_plain_bdf": yerr, "ensemble_members": len(nets),
-                  "train_cells": args.train_cells, "train_steps_per_member": args.train_steps,
-                  "train_seconds": train_s, "gpu_launches": hlaunch,
-                  "mlp_forward": {"ms": mlp_ms, "tflops": mlp_flops / (mlp_ms * 1e-3) / 1e12,
-                                  "bf16_peak_tflops": bf16_peak,
-                                  "frac": (mlp_flops / (mlp_ms * 1e-3) / 1e12 / bf16_peak) if bf16_peak else None,
-                                  "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops)"}}
-        # the headline is the faster of the two integrators that meets the
-        # 1e-4 temperature bar (the plain BDF always does: it is the reference)
-        if terr <= 1e-4 and hybrid["value"] > value:
-            value = hybrid["value"]
+            h.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=dt)  # gate counts
+            hT, hY = T.clone(), rY.clone()
+            last = dict(h.last)
+            hk = args.steps if dt == field.dt else k2
+            l0 = r.kernel_launches()
+            hms_list = time_steps(hstep, restore, hk, 2 if dt != field.dt else args.warmup, stream, barrier)
+            hl = (r.kernel_launches() - l0) * hk // (hk + (2 if dt != field.dt else args.warmup))
+            hms = sharding.step_time_max(sum(hms_list) / len(hms_list), dev)
+            e_t = errs(hT, hY, tT, tY)
+            blk["hybrid"] = {"value": world * nc / (hms * 1e-3), "ms_per_step": hms, "steps": hk,
+                             "speedup_vs_plain_gpu_bdf": blk["plain_ms_per_step"] / hms,
+                             "accepted_fraction": last["accepted_fraction"],
+                             "gate": {k: last[k] for k in last if k.startswith("rejected_") or k in
+                                      ("predicted", "accepted")},
+                             "vs_tight": e_t, "vs_plain_gpu_bdf": errs(hT, hY, pT, pY),
+                             "meets_1e-4_T_bar": e_t["max_rel_T"] <= 1e-4, "gpu_launches": hl,
+                             "rule": ens.opts.__dict__}
+            gpu_res["hybrid"] = (hT, hY)
+            if dt == field.dt:
+                hy_headline = (blk["hybrid"], h)
+            else:
+                h.close()
+        if rank == 0 and not args.no_cpu:
+            blk["sample"] = sample_accuracy(mech, args, dt, gpu_res)
+        blocks[f"dt_{dt:g}"] = blk
+    rt.close()
+    hybrid = hy_headline[0] if hy_headline else None
+    # the headline is the faster of the two integrators that meets the 1e-4
+    # temperature bar against the tight solve (the plain BDF does)
+    use_hybrid = hybrid is not None and hybrid["meets_1e-4_T_bar"] and hybrid["value"] > value
+    if use_hybrid:
+        value = hybrid["value"]
 
     # end to end through the public API from pinned host buffers
     e2e = None
@@ -445,13 +501,14 @@ def run_b200(args, rank, world, local_rank):
         dbuf = {k: torch.empty_like(base[k]) for k in host}
         h2d = sum(t.numel() * t.element_size() for t in host.values())
         d2h = sum(t.numel() * t.element_size() for t in out.values()) + fct_h.numel() * 8
+        hy = hy_headline[1] if (use_hybrid and hy_headline) else None
 
         def e2e_step():
             for k in host:
                 dbuf[k].copy_(host[k], non_blocking=True)
-            if hybrid is not None and value == hybrid["value"]:
-                h.react_flat(dbuf["rhoY"], dbuf["frhoY"], dbuf["T"], dbuf["rhoH"], dbuf["frhoH"], fct,
-                             dt_react=field.dt)
+            if hy is not None:
+                hy.react_flat(dbuf["rhoY"], dbuf["frhoY"], dbuf["T"], dbuf["rhoH"], dbuf["frhoH"], fct,
+                              dt_react=field.dt, stats=False)
             else:
                 r.react_flat(dbuf["rhoY"], dbuf["frhoY"], dbuf["T"], dbuf["rhoH"], dbuf["frhoH"], fct,
                              dt_react=field.dt)
@@ -471,22 +528,16 @@ def run_b200(args, rank, world, local_rank):
         ems = e0.elapsed_time(e1) / args.steps
         ems = sharding.step_time_max(ems, dev)
         e2e = {"value": world * nc / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems, "path": "hybrid" if hy is not None else "plain GPU BDF"}
+    if hy_headline:
+        hy_headline[1].close()
 
     # per-kernel profile: one more react of the same field with CUDA events
     # around every launch (kernel by kernel, outside the timed region)
     restore()
-    torch.cuda.nvtx.range_push("kernel_profile_pass")
     r.profile_begin()
     r.react_flat(rY, base["frhoY"], T, rH, base["frhoH"], fct, dt_react=field.dt)
     prof = r.profile_end()
-    torch.cuda.nvtx.range_pop()
-    # accuracy on a seeded sample of the field: the GPU result of this call
-    # against the CPU oracle at the same tolerances and against a tight FP64
-    # solve (rtol 1e-12)
-    accuracy = None
-    if rank == 0 and not args.no_cpu:
-        accuracy = sample_accuracy(mech, field, rY, T, n=2048)
     kernels, tot_ms = {}, sum(v["ms"] for k, v in prof.items() if k != "complete")
     for k in ("start", "rhs", "ctrl", "jac", "gj", "ctrl_setup"):
         v = prof[k]
@@ -499,10 +550,10 @@ def run_b200(args, rank, world, local_rank):
     c_cells = kernels["ctrl"]["cells"] + kernels["ctrl_setup"]["cells"]
     c_bytes = kernels["ctrl"]["bytes"] + kernels["ctrl_setup"]["bytes"]
     hbm_peak, hbm_src = None, None
-    mp = ROOT / "MEASURED_PEAKS.json"
-    if mp.exists():
+    mp_ = ROOT / "MEASURED_PEAKS.json"
+    if mp_.exists():
         try:
-            hbm_peak = json.loads(mp.read_text()).get("hbm_gbs")
+            hbm_peak = json.loads(mp_.read_text()).get("hbm_gbs")
             hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
         except (ValueError, OSError):
             hbm_peak = None
@@ -518,14 +569,14 @@ def run_b200(args, rank, world, local_rank):
             "share_of_react_kernels": c_ms / tot_ms, "profile_complete": prof["complete"],
             "kernels": kernels}
 
-    # FP64 view of the whole react call (algorithmic flops per call)
+    # FP64 view of the whole react call (algorithmic flops per call, exp/log
+    # counted as one flop each and reported separately)
     counts = perfmodel.op_counts(r.flat)
     cn = {k: counters[k] / nc for k in ("nfe", "nje", "nlu", "nst")}
     fl_cell = perfmodel.flops_per_cell(counts, cn["nfe"], cn["nje"], cn["nlu"], cn["nfe"], cn["nst"])
+    exp_cell = cn["nfe"] * counts["rhs_exp"] + cn["nje"] * counts["jac_exp"]
     achieved = fl_cell * nc / (ms * 1e-3) / 1e12
     peak = fp64_peak_tflops(torch, dev)
-    # FP32 view of the inversion kernel: Gauss-Jordan inverse of the n x n
-    # Newton matrix, n^3 multiply-adds per setup
     n1 = N + 1
     gj_ms = kernels["gj"]["ms"]
     gj_tf = kernels["gj"]["cells"] * 2.0 * n1 ** 3 / (gj_ms * 1e-3) / 1e12 if gj_ms else None
@@ -535,10 +586,15 @@ def run_b200(args, rank, world, local_rank):
                          "peak_source": "measured live: cuBLAS SGEMM 8192^3 without TF32, best of 5"}
     roof["fp64_view"] = {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "kernel": "one react call: rk_rhs / rk_ctrl / rk_jac / rk_gj rounds",
+                         "counting": "algorithmic flops from the integrator's per-cell counters; exp/log = 1 flop",
                          "peak_source": "measured live: cuBLAS DGEMM 8192^3 best of 5 (FP64 has no entry in the "
                                         "measured-peaks file)",
-                         "flops_per_cell": fl_cell, "per_cell_counters": cn,
+                         "flops_per_cell": fl_cell, "exp_log_per_cell": exp_cell,
+                         "exp_log_per_s": exp_cell * nc / (ms * 1e-3), "per_cell_counters": cn,
                          "io_bytes_per_call": perfmodel.bytes_per_cell(N) * nc}
+    if hybrid is not None:
+        mlp_flops = 2.0 * ((N + 2 + 15) // 16 * 16 * 256 + 2 * 256 * 256 + 256 * ((N + 1 + 15) // 16 * 16))
+        hybrid["mlp_flops_per_cell_per_member"] = mlp_flops
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu:
@@ -548,21 +604,87 @@ def run_b200(args, rank, world, local_rank):
                          f"BDF on {threads} host threads ({el:.1f} s), extrapolated to cells/s"}
 
     if rank == 0:
-        path = "hybrid" if (hybrid is not None and value == hybrid["value"]) else "plain GPU BDF"
-        cfg["measured_path"] = path
+        path = "hybrid" if use_hybrid else "plain GPU BDF"
         emit({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
               "warmup": args.warmup, "ms_per_step": world * nc / value * 1e3, "higher_is_better": True,
               "scaling": "weak",
               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded flame-like field; synthetic "
-              "drm19-shaped mechanism)", "config": cfg, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+              "drm19-shaped mechanism)", "config": cfg, "measured_path": path,
+              "integrator": HYBRID_INTEGRATOR if use_hybrid else GPU_INTEGRATOR, "launch_tuning": launch_tuning,
+              "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
               "gpu_launches": launches if path != "hybrid" else hybrid["gpu_launches"], "clocks": clk.summary(),
-              "plain_gpu_bdf": plain, "hybrid": hybrid, "accuracy": accuracy,
+              "plain_gpu_bdf": plain, "hybrid": hybrid, "dt_blocks": blocks,
               "counters": {k: int(v) for k, v in counters.items()}})
     r.close()
 
 
 # ------------------------------------------------------ dodecane workloads
 C12 = "synth_c12_53"
+
+
+def _gen_c12_chunk(a):
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    edge, dt, cells = a
+    f = workloads.c12_flame_grf(mechmod.builtin(C12), edge=edge, dt=dt, cells=cells)
+    return f.rhoY, f.T, f.rhoH
+
+
+def c12_grf_field(args, idx):
+    """The dodecane random-field cells `idx`, generated by a pool of host
+    processes for large fields (each cell depends only on its index)."""
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    mech = mechmod.builtin(C12)
+    if len(idx) <= (1 << 18):
+        return workloads.c12_flame_grf(mech, edge=args.edge, dt=args.dt, cells=idx)
+    import multiprocessing as mp
+    parts = np.array_split(np.asarray(idx, dtype=np.int64), 256)
+    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+        out = pool.map(_gen_c12_chunk, [(args.edge, args.dt, p) for p in parts])
+    rhoY = np.concatenate([o[0] for o in out], axis=1)
+    T = np.concatenate([o[1] for o in out])
+    rhoH = np.concatenate([o[2] for o in out])
+    return workloads.Field(mech, rhoY, T, rhoH, np.zeros_like(rhoY), np.zeros_like(T), args.dt, (len(idx),),
+                           "c12_flame_grf")
+
+
+def c12_class_accuracy(mech, flat, work, args, per_class=96):
+    """GPU result against the oracle (rtol 1e-8 / atol 1e-12) and the tight
+    oracle (rtol 1e-12 / atol 1e-20) on seeded samples of each cell class of
+    the random-field flame: cold (T0 < 600 K), igniting (900 <= T0 < 1500 K),
+    burnt (T0 >= 1800 K)."""
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod
+    f = flat[0]
+    T0 = f.T
+    classes = {"cold": T0 < 600.0, "igniting": (T0 >= 900.0) & (T0 < 1500.0), "burnt": T0 >= 1800.0}
+    o = orc.Oracle(mechmod.flatten(mech))
+    rng = np.random.default_rng(20261203)
+    gT_all = work[0]["T"]
+    gY_all = work[0]["rhoY"]
+    out = {}
+    for name, m in classes.items():
+        cand = np.nonzero(m)[0]
+        if cand.size == 0:
+            continue
+        idx = np.sort(rng.choice(cand, min(per_class, cand.size), replace=False))
+        sub = f.subset(idx)
+        kw = dict(max_order=QMAX, max_steps=100000, nthreads=orc.max_threads())
+        ref = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, f.dt, rtol=RTOL, atol=ATOL, **kw)
+        tight = o.react(sub.rhoY, sub.frhoY, sub.T, sub.rhoH, sub.frhoH, f.dt, rtol=1e-12, atol=1e-20, **kw)
+        import torch
+        it = torch.as_tensor(idx, device=gT_all.device)
+        gT = gT_all.index_select(0, it).cpu().numpy()
+        gY = gY_all.index_select(1, it).cpu().numpy()
+        rho = sub.rhoY.sum(axis=0)
+
+        def err(T, Y, RT, RY):
+            return {"max_rel_T": float(np.max(np.abs(T - RT) / RT)),
+                    "max_abs_Y": float(np.max(np.abs(Y - RY).max(axis=0) / rho))}
+        out[name] = {"cells_in_class": int(cand.size), "sample": int(idx.size),
+                     "gpu_vs_oracle": err(gT, gY, ref["T"], ref["rhoY"]),
+                     "gpu_vs_oracle_tight": err(gT, gY, tight["T"], tight["rhoY"]),
+                     "oracle_vs_oracle_tight": err(ref["T"], ref["rhoY"], tight["T"], tight["rhoY"])}
+    return out
 
 
 def run_dodecane(args, rank, world, local_rank):
@@ -584,7 +706,7 @@ def run_dodecane(args, rank, world, local_rank):
     else:
         n_all = args.edge ** 3
         idx = sharding.shard_cells(n_all, rank, world)
-        flat = [workloads.c12_flame_grf(mech, edge=args.edge, dt=args.dt, cells=idx)]
+        flat = [c12_grf_field(args, idx)]
         total = n_all
         wl = f"c12_grf: dodecane random-field flame {args.edge}^3 (T 300-2400 K, Z 0-1), {total} cells"
     cfg = {"workload": wl + f", synth_c12_53 (53 species + T, {mech.n_reactions} reactions), dt_react "
@@ -689,11 +811,18 @@ def run_dodecane(args, rank, world, local_rank):
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{n} seeded cells of the workload, oracle BDF on {threads} host threads ({el:.1f} s), "
                          f"extrapolated to cells/s"}
+    accuracy = None
+    if args.workload == "c12_grf" and not args.no_cpu:
+        # the result of one more react of the field (untimed) against the oracle per cell class
+        restore()
+        step()
+        torch.cuda.synchronize()
+        accuracy = c12_class_accuracy(mech, flat, work, args)
     emit({"metric": f"cells/s per chem step ({args.workload})", "value": total / (ms * 1e-3), "unit": UNIT,
           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
           "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; synthetic "
           "dodecane-shaped mechanism)", "config": cfg, "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches,
-          "clocks": clk.summary(), "step_ms": step_ms,
+          "clocks": clk.summary(), "step_ms": step_ms, "accuracy_by_class": accuracy,
           "counters": {k: int(v) for k, v in counters.items()} if counters else None})
     r.close()
 
@@ -738,6 +867,10 @@ def main():
         else:
             run_reference(args, rank, world)
         return
+    field = None
+    if args.workload == "flame_ch4":
+        # host-side field generation, before any CUDA call (process pool)
+        field = load_field(args)[1]
     if world > 1:
         import datetime
         import torch
@@ -749,7 +882,7 @@ def main():
         if args.workload != "flame_ch4":
             run_dodecane(args, rank, world, local_rank)
         else:
-            run_b200(args, rank, world, local_rank)
+            run_b200(args, rank, world, local_rank, field)
     finally:
         if world > 1:
             import torch.distributed as dist

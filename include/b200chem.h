@@ -305,6 +305,13 @@ int b200chem_autotune(b200chem_handle h, const double* rhoY, const double* extF_
                       const double* rhoH, const double* extF_rhoH, int64_t ncells, double dt_react,
                       int32_t max_trials, void* stream, b200chem_tuning* best, double* best_ms);
 
+/* Launch-shape cache: writes the handle's tuning to `path` with a header
+ * holding the mechanism digest and the GPU's name and SM count; load sets the
+ * handle's tuning from such a file and fails (B200CHEM_EINVAL, the reason in
+ * b200chem_last_error) when it was made for another mechanism or GPU. */
+int b200chem_tuning_save(b200chem_handle h, const char* path);
+int b200chem_tuning_load(b200chem_handle h, const char* path);
+
 /* Failure detection self-test (no reference counterpart): launches one
  * thread that waits, with the bounded polling loop of the tensor-core
  * kernels, on an mbarrier nothing arrives at; after `polls` polls (1..2^22)
@@ -479,6 +486,15 @@ int b200chem_react_hybrid(b200chem_handle h, b200chem_surrogate_handle s, const 
                           double* rhoY, const double* extF_rhoY, double* T, double* rhoH, const double* extF_rhoH,
                           double* fctCount, const int32_t* mask, int64_t ncells, double* dt_react, double* time,
                           void* stream, int32_t* cell_status, b200chem_stats* stats, b200chem_hybrid_stats* hstats);
+
+/* Surrogate-first form of b200chem_react (box views with ghost cells, call
+ * site Source/PeleLMeX_Reactions.cpp:101-108): the boxes' cells are packed
+ * into the surrogate's flat arrays, reacted by b200chem_react_hybrid and
+ * written back.  cell_status in box order as for b200chem_react. */
+int b200chem_react_hybrid_boxes(b200chem_handle h, b200chem_surrogate_handle s, const b200chem_hybrid_opts* opts,
+                                const b200chem_box_view* boxes, int32_t nbox, double* dt_react, double* time,
+                                void* stream, int32_t* cell_status, b200chem_stats* stats,
+                                b200chem_hybrid_stats* hstats);
 
 #ifdef __cplusplus
 }

@@ -7,8 +7,14 @@
 //
 // Header-only; include it in one translation unit of the PelePhysics build
 // (Reactions/), link -lb200chem.  The mechanism tables come from
-// b200chem_make_mech_desc(), which the build supplies from the CEPTR
-// mechanism in use (the same data pelelmex_b200.mechanism.flatten writes).
+// b200chem_make_mech_desc(), the translation unit that
+//   python -m pelelmex_b200.mechgen --mech-desc <mechanism> --out mech_desc.cpp
+// writes for the mechanism in use.
+//
+// Input keys (besides the reference's ode.rtol, ode.atol, cvode.max_order,
+// cvode.max_substeps): b200.lu_fp64, b200.kernel, and b200.surrogate =
+// <weights file>, which selects the surrogate-first hybrid react
+// (b200chem_react_hybrid_boxes) with the acceptance rule stored in the file.
 #pragma once
 
 #include <string>
@@ -72,7 +78,19 @@ public:
     const b200chem_mech_desc d = b200chem_make_mech_desc();
     h_ = b200chem_create(&d, &o);
     if (!h_) amrex::Abort(b200chem_last_error());
+    std::string weights;
+    pb.query("surrogate", weights);
+    if (!weights.empty()) {
+      sur_ = b200chem_surrogate_load_file(h_, weights.c_str());
+      if (!sur_) amrex::Abort(b200chem_last_error());
+    }
     return 0;
+  }
+
+  // The library takes its thermodynamics from the mechanism description
+  // (ideal gas, NASA-7), so the EOS parameters are kept but not read.
+  void set_eos_parm(const pele::physics::eos::EosParm<pele::physics::PhysicsType::eos_type>* p) override {
+    eos_parm_ = p;
   }
 
   void set_typ_vals_ode(const std::vector<amrex::Real>& v) override {
@@ -85,16 +103,23 @@ public:
             amrex::Array4<int> const& mask, amrex::Real& dt_react, amrex::Real& time,
             amrex::gpuStream_t stream) override {
     const b200chem_box_view v = box_view(box, rY, rYsrc, T, rE, rEsrc, fc, mask);
+    void* st = reinterpret_cast<void*>(stream);
     // the reference aborts the run when its integrator fails
-    if (b200chem_react(h_, &v, 1, &dt_react, &time, reinterpret_cast<void*>(stream), nullptr, nullptr) != 0)
-      amrex::Abort(b200chem_last_error());
+    const int rc = sur_ ? b200chem_react_hybrid_boxes(h_, sur_, nullptr, &v, 1, &dt_react, &time, st, nullptr,
+                                                      nullptr, nullptr)
+                        : b200chem_react(h_, &v, 1, &dt_react, &time, st, nullptr, nullptr);
+    if (rc != 0) amrex::Abort(b200chem_last_error());
     return 0;
   }
 
   void close() override {
+    b200chem_surrogate_destroy(sur_);
+    sur_ = nullptr;
     b200chem_destroy(h_);
     h_ = nullptr;
   }
+
+  bool hybrid() const { return sur_ != nullptr; }
 
   // The b200chem view of one react call's box and fabs.
   static b200chem_box_view box_view(const amrex::Box& box, amrex::Array4<amrex::Real> const& rY,
@@ -118,6 +143,8 @@ public:
 
 private:
   b200chem_handle h_ = nullptr;
+  b200chem_surrogate_handle sur_ = nullptr;
+  const pele::physics::eos::EosParm<pele::physics::PhysicsType::eos_type>* eos_parm_ = nullptr;
 };
 
 }  // namespace pele::physics::reactions

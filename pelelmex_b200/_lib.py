@@ -170,8 +170,10 @@ def load(path: os.PathLike | None = None):
     L.b200chem_selftest_bounded_wait.restype = ctypes.c_int
     L.b200chem_profile_begin.argtypes = [ctypes.c_void_p]
     L.b200chem_profile_end.argtypes = [ctypes.c_void_p, ctypes.POINTER(KernelProfile)]
+    L.b200chem_tuning_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.b200chem_tuning_load.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
     for name in ("b200chem_get_tuning", "b200chem_set_tuning", "b200chem_autotune", "b200chem_profile_begin",
-                 "b200chem_profile_end"):
+                 "b200chem_profile_end", "b200chem_tuning_save", "b200chem_tuning_load"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("b200chem_eval_rhs", "b200chem_eval_jac"):
         f = getattr(L, name)

@@ -1422,6 +1422,69 @@ int b200chem_set_tuning(b200chem_handle h, const b200chem_tuning* t) {
   return 0;
 }
 
+// Tuning cache file: "B2CHTUNE", u32 version (1), u32 header bytes (128),
+// u64 mechanism digest, char[64] GPU name, i32 SM count, i32 reserved, then
+// the b200chem_tuning struct.  A launch shape is kept per (mechanism, GPU).
+namespace {
+constexpr char kTuneMagic[8] = {'B', '2', 'C', 'H', 'T', 'U', 'N', 'E'};
+constexpr uint32_t kTuneVersion = 1, kTuneHeader = 128;
+
+struct TuneHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  uint64_t digest;
+  char gpu[64];
+  int32_t sm_count, reserved;
+  unsigned char pad[kTuneHeader - 8 - 8 - 8 - 64 - 8];
+};
+static_assert(sizeof(TuneHeader) == kTuneHeader, "tuning header layout");
+
+int tune_header(b200chem_handle h, TuneHeader* t) {
+  memset(t, 0, sizeof(*t));
+  memcpy(t->magic, kTuneMagic, 8);
+  t->version = kTuneVersion;
+  t->header_bytes = kTuneHeader;
+  t->digest = h->digest;
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, h->device));
+  snprintf(t->gpu, sizeof(t->gpu), "%s", prop.name);
+  t->sm_count = h->sm_count;
+  return 0;
+}
+}  // namespace
+
+int b200chem_tuning_save(b200chem_handle h, const char* path) {
+  if (!h || !path) return set_err(B200CHEM_EINVAL, "bad arguments");
+  TuneHeader t;
+  int err = tune_header(h, &t);
+  if (err) return err;
+  FILE* f = fopen(path, "wb");
+  if (!f) return set_err(B200CHEM_EINVAL, "cannot write %s", path);
+  const bool ok = fwrite(&t, sizeof(t), 1, f) == 1 && fwrite(&h->tune, sizeof(h->tune), 1, f) == 1;
+  fclose(f);
+  return ok ? 0 : set_err(B200CHEM_EINVAL, "short write to %s", path);
+}
+
+int b200chem_tuning_load(b200chem_handle h, const char* path) {
+  if (!h || !path) return set_err(B200CHEM_EINVAL, "bad arguments");
+  FILE* f = fopen(path, "rb");
+  if (!f) return set_err(B200CHEM_EINVAL, "cannot open %s", path);
+  TuneHeader t, mine;
+  b200chem_tuning tu;
+  const bool ok = fread(&t, sizeof(t), 1, f) == 1 && fread(&tu, sizeof(tu), 1, f) == 1;
+  fclose(f);
+  if (!ok || memcmp(t.magic, kTuneMagic, 8) != 0 || t.version != kTuneVersion || t.header_bytes != kTuneHeader)
+    return set_err(B200CHEM_EINVAL, "%s is not a tuning file of this version", path);
+  int err = tune_header(h, &mine);
+  if (err) return err;
+  if (t.digest != mine.digest) return set_err(B200CHEM_EINVAL, "%s was tuned for another mechanism", path);
+  if (strncmp(t.gpu, mine.gpu, sizeof(t.gpu)) != 0 || t.sm_count != mine.sm_count)
+    return set_err(B200CHEM_EINVAL, "%s was tuned on another GPU (%s)", path, t.gpu);
+  if (!tuning_valid(tu)) return set_err(B200CHEM_EINVAL, "%s holds an invalid launch shape", path);
+  h->tune = tu;
+  return 0;
+}
+
 // Autotuner of the round-based integrator's launch shape.  Each trial copies
 // the sample into work arrays, runs one react over them between two events
 // and reads the elapsed time; coordinate descent over the tuning fields keeps

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
       // constraint rows: the elements (mol of element per gram of species),
       // then the energy at T1 (erg per gram), each scaled to unit max-norm
       const int ne = P.ne < kMaxElem ? P.ne : kMaxElem;
-      double res[kMaxElem + 1], rsc[kMaxElem + 1];
+      double res[kMaxElem + 1], rsc[kMaxElem + 1], tgt[kMaxElem + 1];
       double hk[NS];
       const double rhoH1 = P.rhoH[c] + P.dt * F[NS];
       if (!reason) {
@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
             mx = fmax(mx, fabs(a));
           }
           res[e] = cz - ct;
+          tgt[e] = ct;
           rsc[e] = mx > 0.0 ? 1.0 / mx : 0.0;
           tot += ct;
           worst = fmax(worst, fabs(res[e]));
@@ -303,68 +304,88 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
       if (!reason) {
         // species enthalpies at T1 and the energy row
         const double lnT1 = log(T1);
-        double ez = 0.0, mx = 0.0;
+        double mx = 0.0;
 #pragma unroll
         for (int k = 0; k < NS; ++k) {
           double cpR, hRT, sR, dcpR;
           nasa7(m, k, T1, lnT1, cpR, hRT, sR, dcpR);
           hk[k] = hRT * kRu * T1 * __ldg(m.inv_mw + k);
-          ez += hk[k] * z[k];
           mx = fmax(mx, fabs(hk[k]));
         }
-        res[ne] = ez - rhoH1;
+        tgt[ne] = rhoH1;
         rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
-        // weighted minimum-norm correction: z' = z - D A^T (A D A^T)^-1 (A z - b)
-        // over the ne + 1 scaled rows A (zero rows are skipped)
+        // weighted minimum-norm correction z' = z - W A^T (A W A^T)^-1 (A z - b)
+        // over the ne + 1 scaled rows A (zero rows are skipped).  Pass 0:
+        // W = max(|z_k|, 1e-10 rho).  Partial densities it leaves slightly
+        // negative are set to zero and frozen (W_k = 0) for pass 1, which
+        // restores the constraints exactly without moving them.
         const int nr = ne + 1;
-        double G[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
         auto row = [&](int e, int k) -> double {
           return (e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k]) * rsc[e];
         };
-        for (int e = 0; e < nr; ++e) {
-          lam[e] = res[e] * rsc[e];
-          for (int f = 0; f < nr; ++f) {
-            double g = 0.0;
-            for (int k = 0; k < NS; ++k) g += row(e, k) * row(f, k) * fmax(fabs(z[k]), 1e-10 * rho0);
-            G[e][f] = g;
-          }
-        }
-        // Gauss-Jordan with partial pivoting (singular pivots: row skipped)
-        for (int col = 0; col < nr; ++col) {
-          int piv = col;
-          for (int w = col + 1; w < nr; ++w)
-            if (fabs(G[w][col]) > fabs(G[piv][col])) piv = w;
-          if (!(fabs(G[piv][col]) > 1e-300)) continue;
-          if (piv != col) {
-            for (int w = 0; w < nr; ++w) {
-              const double t = G[col][w];
-              G[col][w] = G[piv][w];
-              G[piv][w] = t;
+        bool frozen_any = false;
+        unsigned long long frozen[(NS + 63) / 64] = {};
+        for (int pass = 0; pass < 2 && !reason; ++pass) {
+          if (pass == 1 && !frozen_any) break;
+          double wk[NS];
+#pragma unroll
+          for (int k = 0; k < NS; ++k)
+            wk[k] = ((frozen[k >> 6] >> (k & 63)) & 1ull) ? 0.0 : fmax(fabs(z[k]), 1e-10 * rho0);
+          double G[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
+          for (int e = 0; e < nr; ++e) {
+            double az = 0.0;
+            for (int k = 0; k < NS; ++k) az += (e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k]) * z[k];
+            res[e] = az - tgt[e];
+            lam[e] = res[e] * rsc[e];
+            for (int f = 0; f < nr; ++f) {
+              double g = 0.0;
+              for (int k = 0; k < NS; ++k) g += row(e, k) * row(f, k) * wk[k];
+              G[e][f] = g;
             }
-            const double t = lam[col];
-            lam[col] = lam[piv];
-            lam[piv] = t;
           }
-          const double inv = 1.0 / G[col][col];
-          for (int w = 0; w < nr; ++w) {
-            if (w == col) continue;
-            const double f = G[w][col] * inv;
-            if (f == 0.0) continue;
-            for (int v = col; v < nr; ++v) G[w][v] -= f * G[col][v];
-            lam[w] -= f * lam[col];
+          // Gauss-Jordan with partial pivoting (singular pivots: row skipped)
+          for (int col = 0; col < nr; ++col) {
+            int piv = col;
+            for (int w = col + 1; w < nr; ++w)
+              if (fabs(G[w][col]) > fabs(G[piv][col])) piv = w;
+            if (!(fabs(G[piv][col]) > 1e-300)) continue;
+            if (piv != col) {
+              for (int w = 0; w < nr; ++w) {
+                const double t = G[col][w];
+                G[col][w] = G[piv][w];
+                G[piv][w] = t;
+              }
+              const double t = lam[col];
+              lam[col] = lam[piv];
+              lam[piv] = t;
+            }
+            const double inv = 1.0 / G[col][col];
+            for (int w = 0; w < nr; ++w) {
+              if (w == col) continue;
+              const double f = G[w][col] * inv;
+              if (f == 0.0) continue;
+              for (int v = col; v < nr; ++v) G[w][v] -= f * G[col][v];
+              lam[w] -= f * lam[col];
+            }
           }
-        }
-        for (int e = 0; e < nr; ++e) lam[e] = (fabs(G[e][e]) > 1e-300) ? lam[e] / G[e][e] : 0.0;
+          for (int e = 0; e < nr; ++e) lam[e] = (fabs(G[e][e]) > 1e-300) ? lam[e] / G[e][e] : 0.0;
 #pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          double corr = 0.0;
-          for (int e = 0; e < nr; ++e) corr += row(e, k) * lam[e];
-          z[k] -= fmax(fabs(z[k]), 1e-10 * rho0) * corr;
-        }
+          for (int k = 0; k < NS; ++k) {
+            double corr = 0.0;
+            for (int e = 0; e < nr; ++e) corr += row(e, k) * lam[e];
+            z[k] -= wk[k] * corr;
+          }
 #pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          if (z[k] < -P.o.tol_mass * rho1t) reason = kRejNegative;
-          z[k] = fmax(z[k], 0.0);
+          for (int k = 0; k < NS; ++k) {
+            if (z[k] < -P.o.tol_mass * rho1t) reason = kRejNegative;
+            if (z[k] < 0.0) {
+              z[k] = 0.0;
+              if (pass == 0) {
+                frozen[k >> 6] |= 1ull << (k & 63);
+                frozen_any = true;
+              }
+            }
+          }
         }
       }
       if (!reason && P.o.resid > 0.0) {
@@ -523,6 +544,8 @@ struct b200chem_surrogate {
   void* d_hy = nullptr;         // hybrid scratch: reject list, counters, compact state
   size_t hy_bytes = 0;
   int* h_count = nullptr;       // pinned: rejected count, GEMM error flag
+  void* d_pack = nullptr;       // packed box-view state of b200chem_react_hybrid_boxes
+  size_t pack_bytes = 0;
   cudaStream_t last_stream = nullptr;
 };
 
@@ -774,6 +797,7 @@ extern "C" int b200chem_surrogate_destroy(b200chem_surrogate_handle s) {
   if (s->d_params) cudaFree(s->d_params);
   if (s->d_scratch) cudaFree(s->d_scratch);
   if (s->d_hy) cudaFree(s->d_hy);
+  if (s->d_pack) cudaFree(s->d_pack);
   if (s->h_count) cudaFreeHost(s->h_count);
   delete s;
   return 0;
@@ -966,4 +990,164 @@ extern "C" int b200chem_surrogate_features(b200chem_handle h, const double* rhoY
   if (err) return handle_set_error(err, "surrogate_features: launch failed");
   handle_count_launch(h);
   return 0;
+}
+
+// ------------------------------------------------ hybrid react on box views
+namespace b200 {
+namespace {
+
+// One box of b200chem_react_hybrid_boxes: its Array4 views and its first
+// cell in the packed (flat, component-major) order.
+struct HyBox {
+  int lo0, lo1, lo2, nx, ny, nz;
+  long long off;
+  DevArr rY, fY, T, rH, fH, fc;
+  DevIArr mask;
+};
+
+__device__ __forceinline__ int hy_locate(const HyBox* boxes, int nbox, long long cell, int* i, int* j, int* k) {
+  int lo = 0, hi = nbox - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (boxes[mid].off <= cell) lo = mid;
+    else hi = mid - 1;
+  }
+  const HyBox& b = boxes[lo];
+  const long long loc = cell - b.off;
+  *i = b.lo0 + (int)(loc % b.nx);
+  *j = b.lo1 + (int)((loc / b.nx) % b.ny);
+  *k = b.lo2 + (int)(loc / ((long long)b.nx * b.ny));
+  return lo;
+}
+
+// phase 0: Array4 views -> packed arrays (state, forcing, mask); phase 1:
+// packed results -> Array4 views (rhoY, T, rhoH, fctCount)
+__global__ void hy_pack(const HyBox* __restrict__ boxes, int nbox, long long total, int N, int phase, double* pY,
+                        double* pfY, double* pT, double* pH, double* pfH, double* pfc, int* pm) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    const HyBox& b = boxes[hy_locate(boxes, nbox, c, &i, &j, &k)];
+    if (phase == 0) {
+      for (int n = 0; n < N; ++n) {
+        pY[n * total + c] = elem(b.rY, i, j, k)[n * b.rY.ns];
+        pfY[n * total + c] = elem(b.fY, i, j, k)[n * b.fY.ns];
+      }
+      pT[c] = *elem(b.T, i, j, k);
+      pH[c] = *elem(b.rH, i, j, k);
+      pfH[c] = *elem(b.fH, i, j, k);
+      pm[c] = b.mask.p ? b.mask.p[(long long)(i - b.mask.lo0) + (long long)(j - b.mask.lo1) * b.mask.js +
+                                  (long long)(k - b.mask.lo2) * b.mask.ks]
+                       : 1;
+    } else {
+      for (int n = 0; n < N; ++n) elem(b.rY, i, j, k)[n * b.rY.ns] = pY[n * total + c];
+      *elem(b.T, i, j, k) = pT[c];
+      *elem(b.rH, i, j, k) = pH[c];
+      if (b.fc.p) *elem(b.fc, i, j, k) = pfc[c];
+    }
+  }
+}
+
+DevArr view_dev(const b200chem_array4& a) {
+  DevArr d;
+  d.p = a.p;
+  d.js = a.jstride;
+  d.ks = a.kstride;
+  d.ns = a.nstride;
+  d.lo0 = a.lo[0];
+  d.lo1 = a.lo[1];
+  d.lo2 = a.lo[2];
+  d.pad = 0;
+  return d;
+}
+
+}  // namespace
+}  // namespace b200
+
+extern "C" int b200chem_react_hybrid_boxes(b200chem_handle h, b200chem_surrogate_handle s,
+                                           const b200chem_hybrid_opts* opts, const b200chem_box_view* views,
+                                           int32_t nbox, double* dt_react, double* time, void* stream,
+                                           int32_t* cell_status, b200chem_stats* stats,
+                                           b200chem_hybrid_stats* hstats) {
+  if (!h || !s || (!views && nbox > 0) || nbox < 0 || !dt_react)
+    return sur_err(B200CHEM_EINVAL, "react_hybrid_boxes: bad arguments");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::vector<HyBox> hb(nbox);
+  long long total = 0;
+  for (int b = 0; b < nbox; ++b) {
+    const b200chem_box_view& v = views[b];
+    if (!v.rhoY.p || !v.extF_rhoY.p || !v.T.p || !v.rhoH.p || !v.extF_rhoH.p)
+      return sur_err(B200CHEM_EINVAL, "react_hybrid_boxes: null state array");
+    HyBox& d = hb[b];
+    d.lo0 = v.lo[0];
+    d.lo1 = v.lo[1];
+    d.lo2 = v.lo[2];
+    d.nx = v.hi[0] - v.lo[0] + 1;
+    d.ny = v.hi[1] - v.lo[1] + 1;
+    d.nz = v.hi[2] - v.lo[2] + 1;
+    if (d.nx < 1 || d.ny < 1 || d.nz < 1) return sur_err(B200CHEM_EINVAL, "react_hybrid_boxes: empty box");
+    d.off = total;
+    total += (long long)d.nx * d.ny * d.nz;
+    d.rY = view_dev(v.rhoY);
+    d.fY = view_dev(v.extF_rhoY);
+    d.T = view_dev(v.T);
+    d.rH = view_dev(v.rhoH);
+    d.fH = view_dev(v.extF_rhoH);
+    d.fc = view_dev(v.fctCount);
+    d.mask.p = v.mask.p;
+    d.mask.js = v.mask.jstride;
+    d.mask.ks = v.mask.kstride;
+    d.mask.lo0 = v.mask.lo[0];
+    d.mask.lo1 = v.mask.lo[1];
+    d.mask.lo2 = v.mask.lo[2];
+    d.mask.pad = 0;
+  }
+  if (total == 0) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (hstats) memset(hstats, 0, sizeof(*hstats));
+    if (time) *time += *dt_react;
+    return 0;
+  }
+  if (total > 0x7fffffffLL) return sur_err(B200CHEM_ETOOBIG, "react_hybrid_boxes: more than 2^31-1 cells");
+  // packed arrays and the box descriptors in one allocation, owned by the
+  // surrogate and reused across calls
+  const int N = s->N;
+  const size_t desc_b = align256(sizeof(HyBox) * (size_t)nbox);
+  const size_t need = desc_b + align256(8 * (size_t)total * (2 * N + 4)) + align256(4 * (size_t)total);
+  if (need > s->pack_bytes) {
+    if (s->d_pack) {
+      SCK(cudaStreamSynchronize(st));
+      cudaFree(s->d_pack);
+      s->d_pack = nullptr;
+      s->pack_bytes = 0;
+    }
+    if (cudaMalloc(&s->d_pack, need) != cudaSuccess) {
+      cudaGetLastError();
+      return sur_err(B200CHEM_ENOMEM, "react_hybrid_boxes: cannot allocate the packed arrays");
+    }
+    s->pack_bytes = need;
+  }
+  unsigned char* q = static_cast<unsigned char*>(s->d_pack);
+  HyBox* d_boxes = reinterpret_cast<HyBox*>(q);
+  double* pY = reinterpret_cast<double*>(q + desc_b);
+  double* pfY = pY + (size_t)N * total;
+  double* pT = pfY + (size_t)N * total;
+  double* pH = pT + total;
+  double* pfH = pH + total;
+  double* pfc = pfH + total;
+  int* pm = reinterpret_cast<int*>(q + desc_b + align256(8 * (size_t)total * (2 * N + 4)));
+  // the descriptors are copied synchronously from host memory (small)
+  SCK(cudaMemcpyAsync(d_boxes, hb.data(), sizeof(HyBox) * (size_t)nbox, cudaMemcpyHostToDevice, st));
+  SCK(cudaStreamSynchronize(st));
+  const long long blocks = std::min<long long>((total + 255) / 256, 8LL * handle_sm_count(h));
+  hy_pack<<<(unsigned)blocks, 256, 0, st>>>(d_boxes, nbox, total, N, 0, pY, pfY, pT, pH, pfH, pfc, pm);
+  SCK(cudaGetLastError());
+  handle_count_launch(h);
+  int rc = b200chem_react_hybrid(h, s, opts, pY, pfY, pT, pH, pfH, pfc, pm, total, dt_react, time, stream,
+                                 cell_status, stats, hstats);
+  if (rc != 0 && rc != B200CHEM_EINTEGRATE) return rc;
+  hy_pack<<<(unsigned)blocks, 256, 0, st>>>(d_boxes, nbox, total, N, 1, pY, pfY, pT, pH, pfH, pfc, pm);
+  SCK(cudaGetLastError());
+  handle_count_launch(h);
+  return rc;
 }

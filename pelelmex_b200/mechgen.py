@@ -184,3 +184,57 @@ def generate_bundled() -> str:
         parts.append(generate(flat, name))
     parts += ["}  // namespace gen", "}  // namespace b200"]
     return "\n".join(parts) + "\n"
+
+
+def _c_array(ctype: str, name: str, values, per_line: int = 6) -> str:
+    vals = [repr(float(v)) if ctype == "double" else str(int(v)) for v in np.ravel(values)]
+    if not vals:
+        vals = ["0"]
+    lines = [", ".join(vals[i:i + per_line]) for i in range(0, len(vals), per_line)]
+    return f"static const {ctype} {name}[{len(vals)}] = {{\n  " + ",\n  ".join(lines) + "\n};\n"
+
+
+def generate_mech_desc(flat, name: str) -> str:
+    """C++ translation unit defining b200chem_make_mech_desc() for one
+    mechanism: the flat description (the data a CEPTR-generated mechanism
+    bakes into code) as static tables, so a PelePhysics build links the
+    ReactorB200 shim without hand-written mechanism code.  The digest it
+    carries in a comment is the one the library computes for it."""
+    a = flat.arrays
+    ne = flat.n_eff
+    out = [f"// b200chem mechanism description of {name}: {flat.n_species} species, {flat.n_reactions} "
+           f"reactions.", "// Generated by pelelmex_b200.mechgen; do not edit.",
+           f"// digest 0x{mechanism_digest(flat):016x}", '#include "b200chem.h"', "", "namespace {"]
+    for key, ct in (("mw", "double"), ("nasa", "double"), ("rtype", "int32_t"), ("rflags", "int32_t"),
+                    ("arr", "double"), ("arr_lo", "double"), ("arr_rev", "double"), ("troe", "double"),
+                    ("sp", "int32_t"), ("nu", "int32_t"), ("eff_ptr", "int32_t")):
+        out.append(_c_array(ct, f"k_{key}", a[key]))
+    out.append(_c_array("int32_t", "k_eff_sp", a["eff_sp"][:max(ne, 0)]))
+    out.append(_c_array("double", "k_eff_val", a["eff_val"][:max(ne, 0)]))
+    out += ["}  // namespace", "", "b200chem_mech_desc b200chem_make_mech_desc() {", "  b200chem_mech_desc d{};",
+            f"  d.n_species = {flat.n_species};", f"  d.n_reactions = {flat.n_reactions};", f"  d.n_eff = {ne};"]
+    for key in ("mw", "nasa", "rtype", "rflags", "arr", "arr_lo", "arr_rev", "troe", "sp", "nu", "eff_ptr",
+                "eff_sp", "eff_val"):
+        out.append(f"  d.{key} = k_{key};")
+    out += ["  return d;", "}", ""]
+    return "\n".join(out)
+
+
+def main(argv=None):
+    """python -m pelelmex_b200.mechgen --mech-desc MECHANISM --out FILE.cpp
+
+    MECHANISM is a bundled mechanism name or a Cantera-style YAML file."""
+    import argparse
+    from pathlib import Path
+    from . import mechanism as mechmod
+    p = argparse.ArgumentParser()
+    p.add_argument("--mech-desc", required=True)
+    p.add_argument("--out", required=True)
+    a = p.parse_args(argv)
+    src = a.mech_desc
+    mech = mechmod.load(src) if Path(src).exists() else mechmod.builtin(src)
+    Path(a.out).write_text(generate_mech_desc(mechmod.flatten(mech), mech.name if hasattr(mech, "name") else src))
+
+
+if __name__ == "__main__":
+    main()

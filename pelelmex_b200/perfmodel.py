@@ -10,8 +10,8 @@ PelePhysics Reactions/ReactorCvode.cpp, as printed by the reference at
 Source/PeleLMeX_Reactions.cpp:122-141 when fctCount is requested).
 
 Counting rules (one add, mul or compare = 1 flop; an FMA = 2; a division or
-square root = 1; exp / log / log10 / pow = EXP_FLOPS each, the cost of a
-range reduction plus a degree-11 polynomial):
+square root = 1; an exp / log / log10 / pow = 1 flop, and the number of them
+is reported separately, "EXP" below):
 
 * thermo per species: NASA-7 cp/R, h/RT, s/R, g/RT by Horner       -> 30
 * concentration C_k = rhoY_k / W_k                                   -> 1
@@ -34,11 +34,13 @@ from __future__ import annotations
 
 import numpy as np
 
-EXP_FLOPS = 24
+EXP_FLOPS = 1
 
 
 def op_counts(flat) -> dict:
-    """Per-call FP64 flop counts for one cell of the flattened mechanism."""
+    """Per-call FP64 flop counts for one cell of the flattened mechanism
+    (exp/log counted as one flop each), with the number of exp/log calls of
+    one right-hand side and one Jacobian in rhs_exp / jac_exp."""
     a = flat.arrays
     N, R = flat.n_species, flat.n_reactions
     n = N + 1
@@ -49,20 +51,27 @@ def op_counts(flat) -> dict:
     rx = 0
     jac_extra = 0
     nnz = 0
+    n_exp = 1  # log T
     for j in range(R):
         slots = [s for s in range(8) if sp[j, s] >= 0]
         neff = int(eff_ptr[j + 1] - eff_ptr[j])
         c = 4 + EXP_FLOPS
+        e = 1
         if rtype[j] != 0:
             c += 2 * neff + 1
         if rtype[j] >= 2:
             c += 8 + EXP_FLOPS
+            e += 1
         if rtype[j] == 3:
             c += 20 + 6 * EXP_FLOPS
+            e += 6
         if rflags[j] & 2:
             c += 4 + EXP_FLOPS
+            e += 1
         elif rflags[j] & 1:
             c += 2 * len(slots) + 4 + EXP_FLOPS
+            e += 1
+        n_exp += e
         c += int(np.abs(nu[j, slots]).sum()) + 3
         rx += c
         nnz += len(set(int(sp[j, s]) for s in slots))
@@ -74,7 +83,8 @@ def op_counts(flat) -> dict:
     jac = rhs + jac_extra + n * 2 * N
     lu = (2 * n ** 3) // 3
     solve = 2 * n * n
-    return dict(n=n, rhs=rhs, jac=jac, lu=lu, solve=solve, refine=2 * n * n + solve)
+    return dict(n=n, rhs=rhs, jac=jac, lu=lu, solve=solve, refine=2 * n * n + solve, rhs_exp=n_exp,
+                jac_exp=n_exp)
 
 
 def flops_per_cell(counts: dict, nfe: float, nje: float, nlu: float, nni: float, nst: float) -> float:

@@ -209,6 +209,20 @@ class ReactorB200:
             float(dt_react), int(max_trials), _stream_ptr(stream), ctypes.byref(best), ctypes.byref(ms)))
         return {f: int(getattr(best, f)) for f in self.TUNING_FIELDS}, float(ms.value)
 
+    def save_tuning(self, path):
+        """Writes the launch shape to a cache file keyed by mechanism and GPU."""
+        self._need()
+        _lib.check(_lib.load().b200chem_tuning_save(self._h, str(path).encode()))
+
+    def load_tuning(self, path) -> bool:
+        """Sets the launch shape from a cache file; False (and the shape
+        unchanged) when the file is missing or was made for another
+        mechanism or GPU."""
+        self._need()
+        if not Path(path).exists():
+            return False
+        return _lib.load().b200chem_tuning_load(self._h, str(path).encode()) == 0
+
     def profile_begin(self):
         """Per-kernel event timing of the following react calls (round-based
         integrator; kernels are then launched one by one, not from a graph)."""

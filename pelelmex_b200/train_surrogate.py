@@ -14,7 +14,8 @@
    field at both time steps and the largest temperature error of an accepted
    cell against the plain BDF is measured; the most permissive rule whose
    worst accepted cell stays within `margin` of the 1e-4 bar at both time
-   steps is kept (the candidates are ordered from strict to permissive).
+   steps is kept (the candidates are ordered from strict to permissive; if
+   none does, the strictest is stored and the report says so).
 4. The versioned weights file (the format of b200chem_surrogate_load) carries
    the networks, their normalisation, the element matrix and the rule.
 """
@@ -32,7 +33,7 @@ import numpy as np
 EDGE = 128
 
 # candidate acceptance rules, strict to permissive: (spread, dT_cap, gap) in bars
-CANDIDATES = [(0.03, 5.0, 2.0), (0.05, 5.0, 3.0), (0.05, 10.0, 3.0), (0.08, 10.0, 3.0), (0.1, 10.0, 3.0),
+CANDIDATES = [(0.02, 3.0, 1.5), (0.03, 5.0, 2.0), (0.05, 5.0, 3.0), (0.05, 10.0, 3.0), (0.08, 10.0, 3.0), (0.1, 10.0, 3.0),
               (0.1, 15.0, 3.0), (0.12, 15.0, 3.0), (0.15, 15.0, 3.0), (0.15, 20.0, 3.0), (0.2, 20.0, 5.0)]
 
 
@@ -70,7 +71,7 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
             fct = torch.zeros_like(a[1])
             reactor.react_flat(a[0], fY, a[1], a[2], fH, fct, dt_react=dt)
             plain[(key, dt)] = (a[1], fct)
-    table, best = [], None
+    table, best, worst = [], None, {}
     for spread, cap, gap in CANDIDATES:
         opts = HybridOpts(spread=spread, dT_cap=cap, gap=gap)
         row = {"spread": spread, "dT_cap": cap, "gap": gap}
@@ -82,17 +83,29 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
                 h = HybridReactor(reactor, ens, opts)
                 h.react_flat(a[0], fY, a[1], a[2], fH, None, dt_react=dt)
                 T_ref, fct = plain[(key, dt)]
-                err = ((a[1] - T_ref).abs() / (opts.t_rel * T_ref)).max().item()
+                e = (a[1] - T_ref) / (opts.t_rel * T_ref)
+                err = e.abs().max().item()
                 acc = h.last["accepted"] / h.last["predicted"]
+                # cost the BDF no longer spends: right-hand sides of the accepted cells
+                hf = torch.zeros_like(fct)
+                a2 = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
+                h.react_flat(a2[0], fY, a2[1], a2[2], fH, hf, dt_react=dt)
+                saved = (fct[hf == 0].sum() / fct.sum()).item()
                 h.close()
-                row[f"{key}_dt{dt:g}"] = {"accepted": round(acc, 4), "max_err_bars": round(err, 4)}
+                row[f"{key}_dt{dt:g}"] = {"accepted": round(acc, 4), "bdf_cost_saved": round(saved, 4),
+                                          "max_err_bars": round(err, 4)}
+                # the worst accepted cells of this rule (cell, x index, T0, error in bars)
+                top = torch.topk(e.abs(), 8)
+                worst[(spread, cap, gap, key, dt)] = [
+                    (int(c), int(c) % EDGE, round(float(T[int(c)]), 1), round(float(e[int(c)]), 3))
+                    for c in top.indices.tolist()]
                 ok_all &= err <= margin
         row["within_margin"] = bool(ok_all)
         table.append(row)
         log(json.dumps(row))
         if ok_all:
             best = opts
-    return best, table
+    return best, table, worst
 
 
 def main():
@@ -102,9 +115,9 @@ def main():
     p.add_argument("--seeds", default="10,11,12,13,14,15", help="training field seeds")
     p.add_argument("--val-seed", type=int, default=5, help="held-out calibration field seed")
     p.add_argument("--members", type=int, default=8)
-    p.add_argument("--steps", type=int, default=12000)
+    p.add_argument("--steps", type=int, default=20000)
     p.add_argument("--batch", type=int, default=16384)
-    p.add_argument("--margin", type=float, default=0.5, help="worst accepted cell allowed, in bars")
+    p.add_argument("--margin", type=float, default=0.75, help="worst accepted cell allowed, in bars")
     p.add_argument("--report", default=None, help="JSON file for the calibration table")
     a = p.parse_args()
     seeds = [int(s) for s in a.seeds.split(",")]
@@ -128,16 +141,27 @@ def main():
     torch.cuda.synchronize()
     print(f"trained {a.members} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
     ens = Ensemble(nets)
-    rule, table = calibrate(r, ens, {f"seed{a.val_seed}": fields[a.val_seed]}, dts, a.margin)
-    if rule is None:
-        raise SystemExit("no candidate acceptance rule keeps the held-out field within the margin")
+    rule, table, worst = calibrate(r, ens, {f"seed{a.val_seed}": fields[a.val_seed]}, dts, a.margin)
+    within = rule is not None
+    if not within:
+        from .surrogate import HybridOpts
+        sp, cap, gap = CANDIDATES[0]
+        rule = HybridOpts(spread=sp, dT_cap=cap, gap=gap)
+        print("WARNING: no candidate rule keeps the held-out field within the margin; storing the strictest",
+              flush=True)
     ens.opts = rule
     ens.save(a.out)
     print(f"saved {a.out}: rule {rule}", flush=True)
+    key = (rule.spread, rule.dT_cap, rule.gap)
+    for (sp, cap, gap, fk, dt), cells in worst.items():
+        if (sp, cap, gap) == key:
+            print(f"worst accepted cells of the rule, {fk} dt {dt:g} (cell, x, T0, error in bars): {cells}",
+                  flush=True)
     if a.report:
         with open(a.report, "w") as f:
-            json.dump({"rule": rule.__dict__, "table": table, "members": a.members, "steps": a.steps,
-                       "train_seeds": seeds, "val_seed": a.val_seed, "dts": dts}, f, indent=1)
+            json.dump({"rule": rule.__dict__, "within_margin": within, "margin_bars": a.margin, "table": table,
+                       "members": a.members, "steps": a.steps, "train_seeds": seeds, "val_seed": a.val_seed,
+                       "dts": dts}, f, indent=1)
     r.close()
 
 

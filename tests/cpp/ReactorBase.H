@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <map>
 #include <memory>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -37,10 +38,23 @@ struct Box {
   int bigEnd(int d) const { return hi[d]; }
 };
 
+// Input keys "prefix.name" -> value, filled by the host program that
+// stands in for the inputs file.
 struct ParmParse {
-  explicit ParmParse(const std::string&) {}
+  explicit ParmParse(const std::string& prefix) : prefix_(prefix) {}
+  static std::map<std::string, std::string>& table() {
+    static std::map<std::string, std::string> t;
+    return t;
+  }
   template <class T>
-  int query(const char*, T&) const { return 0; }
+  int query(const char* name, T& v) const {
+    auto it = table().find(prefix_ + "." + name);
+    if (it == table().end()) return 0;
+    std::istringstream in(it->second);
+    in >> v;
+    return 1;
+  }
+  std::string prefix_;
 };
 
 [[noreturn]] inline void Abort(const char* msg) {
@@ -48,6 +62,17 @@ struct ParmParse {
   std::exit(3);
 }
 }  // namespace amrex
+
+namespace pele::physics {
+struct Fuego {};
+struct PhysicsType {
+  using eos_type = Fuego;
+};
+namespace eos {
+template <class EosType>
+struct EosParm {};
+}  // namespace eos
+}  // namespace pele::physics
 
 namespace pele::physics::reactions {
 // self-registering factory base, in the manner of the one the reference's
@@ -76,6 +101,9 @@ public:
   virtual int init(int reactor_type, int ncells) = 0;
   virtual void close() = 0;
   virtual void set_typ_vals_ode(const std::vector<amrex::Real>& typ) = 0;
+  // Source/PeleLMeX_Setup.cpp:155 passes the EOS parameters after init
+  virtual void set_eos_parm(const eos::EosParm<PhysicsType::eos_type>* eos_parm) { m_eos_parm = eos_parm; }
+  const eos::EosParm<PhysicsType::eos_type>* m_eos_parm = nullptr;
   virtual int react(const amrex::Box& box, amrex::Array4<amrex::Real> const& rY_in,
                     amrex::Array4<amrex::Real> const& rYsrc_in, amrex::Array4<amrex::Real> const& T_in,
                     amrex::Array4<amrex::Real> const& rEner_in, amrex::Array4<amrex::Real> const& rEner_src_in,

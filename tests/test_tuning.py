@@ -135,3 +135,27 @@ def test_kernel_profile_counts_match_integrator_counters():
     torch.cuda.synchronize()
     assert torch.equal(T, T2) and torch.equal(rhoY, rY2)
     r.close()
+
+
+@pytest.mark.gpu
+def test_tuning_cache_round_trip_and_keys(tmp_path):
+    """The launch-shape cache keeps a tuning per (mechanism, GPU): a second
+    handle of the same mechanism loads it; another mechanism is refused."""
+    from pelelmex_b200.reactor import ReactorB200
+    a = ReactorB200("synth_ch4_21", rtol=1e-8, atol=1e-12, max_order=5).init()
+    b = ReactorB200("synth_ch4_21", rtol=1e-8, atol=1e-12, max_order=5).init()
+    c = ReactorB200("synth_h2_9", rtol=1e-8, atol=1e-12, max_order=5).init()
+    try:
+        a.set_tuning(rhs_ctas_per_sm=3, rounds_per_check=8, use_graph=2)
+        path = tmp_path / "ch4.b2t"
+        a.save_tuning(path)
+        assert b.get_tuning() != a.get_tuning()
+        assert b.load_tuning(path)
+        assert b.get_tuning() == a.get_tuning()
+        before = c.get_tuning()
+        assert not c.load_tuning(path)
+        assert c.get_tuning() == before
+        assert not b.load_tuning(tmp_path / "missing.b2t")
+    finally:
+        for r in (a, b, c):
+            r.close()
