@@ -90,7 +90,15 @@ typedef struct b200chem_opts {
   int32_t max_steps;     /* maximum internal steps per cell and call            */
   int32_t reactor_type;  /* 2 = HP (constant pressure, enthalpy forcing); only 2 */
   int32_t lu_fp64;       /* 0: FP32 LU + one FP64 refinement step (default); 1: FP64 LU */
-  int32_t warps_per_cta; /* unused; kept for layout stability (set 0)           */
+  int32_t refine_stall_ppm; /* round-based integrator with the FP32 inverse: a
+                            Newton correction whose FP64 refinement step is
+                            larger (in the WRMS norm) than this many parts per
+                            million of the correction (the FP32 inverse does
+                            not resolve the iteration matrix) stops its cell,
+                            untouched, and the cell is integrated again from
+                            its input by a pass with the FP64 LU in the same
+                            react call; 0 = default (250000, a quarter),
+                            negative = never                                  */
   int32_t verbose;
   int32_t kernel;        /* 0: auto (round-based integrator where the species
                             count has a compiled variant, else the group
@@ -146,6 +154,7 @@ typedef struct b200chem_stats {
   int64_t n_cells, n_masked, n_failed;
   int64_t nst, nfe, nje, nlu, netf, ncfn;
   int32_t max_nfe, max_nst;
+  int64_t n_fp64_retry; /* cells integrated again with the FP64 LU (refine_stall_ppm) */
 } b200chem_stats;
 
 typedef struct b200chem_reactor* b200chem_handle;

@@ -19,7 +19,7 @@ _f64p = ctypes.c_void_p  # device pointers are passed as integers
 class Opts(ctypes.Structure):
     _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_order", ctypes.c_int32),
                 ("max_steps", ctypes.c_int32), ("reactor_type", ctypes.c_int32), ("lu_fp64", ctypes.c_int32),
-                ("warps_per_cta", ctypes.c_int32), ("verbose", ctypes.c_int32), ("kernel", ctypes.c_int32),
+                ("refine_stall_ppm", ctypes.c_int32), ("verbose", ctypes.c_int32), ("kernel", ctypes.c_int32),
                 ("setup_ratio", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
                 ("group_lanes", ctypes.c_int32)]
 
@@ -51,7 +51,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("n_cells", ctypes.c_int64), ("n_masked", ctypes.c_int64), ("n_failed", ctypes.c_int64),
                 ("nst", ctypes.c_int64), ("nfe", ctypes.c_int64), ("nje", ctypes.c_int64), ("nlu", ctypes.c_int64),
                 ("netf", ctypes.c_int64), ("ncfn", ctypes.c_int64), ("max_nfe", ctypes.c_int32),
-                ("max_nst", ctypes.c_int32)]
+                ("max_nst", ctypes.c_int32), ("n_fp64_retry", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -255,6 +255,8 @@ struct b200chem_reactor {
   int rgraph_rounds = 0;              // rounds in rgraph
   StagedBuf cboxes;                   // advanceChemistry box descriptors
   StagedBuf fboxes;                   // getScalarReactForce box descriptors
+  int* d_retry = nullptr;             // per-cell flags of the FP64 fallback pass
+  size_t retry_bytes = 0;
   int* d_zero_mask = nullptr;         // all-zero mask row of the covered (skip_react) boxes
   long long zero_mask_len = 0;
   // per-kernel profile of the round integrator (b200chem_profile_begin/end)
@@ -534,10 +536,10 @@ int capture_rounds(b200chem_reactor* h, int lut, const RoundsParams& R, const Ro
 
 // Round-based integrator: rhs / ctrl / setup kernels over compacted lists,
 // chunk by chunk (see react_rounds.cu).
-int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st) {
+int launch_rounds(b200chem_reactor* h, const ReactParams& P, cudaStream_t st, int force_lut = 0) {
   if (!rounds_supported(h->N))
     return set_err(B200CHEM_EINVAL, "round-based integrator not compiled for N=%d", h->N);
-  const int lut = h->opts.lu_fp64 ? 8 : 4;
+  const int lut = force_lut ? force_lut : (h->opts.lu_fp64 ? 8 : 4);
   const RoundsSetupLayout SL = rounds_setup_layout(h->N, h->R, lut);
   if (4 * std::max(SL.jac_smem_per_warp, SL.gj_smem_per_warp) > h->smem_optin - 2048)
     return set_err(B200CHEM_ETOOBIG, "setup kernels need %d B of shared memory per CTA",
@@ -673,16 +675,41 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   P.queue = h->d_scratch;
   P.stats = reinterpret_cast<long long*>(h->d_scratch + 1);
   P.status = cell_status;
+  P.refine_stall = 0.0;
+  P.retry = nullptr;
+  P.retry_pass = 0;
   if (h->opts.kernel == 1 && !tpc_supported(h->N))
     return set_err(B200CHEM_EINVAL, "thread-per-cell kernel requested but not compiled for N=%d", h->N);
   if (total > 0) {
     // auto: the round-based integrator where its species count is compiled,
     // else the group integrator (any species count)
     const int k = (h->opts.kernel == 0) ? (rounds_supported(h->N) ? 3 : 2) : h->opts.kernel;
-    const int err = (k == 1) ? launch_thread_per_cell(h, P, st)
-                    : (k == 3) ? launch_rounds(h, P, st)
-                               : launch_group(h, P, st);
+    const int ppm = h->opts.refine_stall_ppm;
+    if (k == 3 && !h->opts.lu_fp64 && ppm >= 0) {
+      // per-cell FP64 fallback: flags of the cells whose refined FP32 solve stalls
+      P.refine_stall = (ppm == 0 ? 250000 : ppm) * 1e-6;
+      int err = ensure_buffer(reinterpret_cast<void**>(&h->d_retry), &h->retry_bytes, sizeof(int) * (size_t)total,
+                              st, "FP64-retry flags");
+      if (err) return err;
+      CK(cudaMemsetAsync(h->d_retry, 0, sizeof(int) * (size_t)total, st));
+      P.retry = h->d_retry;
+    }
+    int err = (k == 1) ? launch_thread_per_cell(h, P, st)
+              : (k == 3) ? launch_rounds(h, P, st)
+                         : launch_group(h, P, st);
     if (err) return err;
+    if (P.retry) {
+      long long stalled = 0;
+      CK(cudaMemcpyAsync(&stalled, P.stats + kStStall, sizeof(long long), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (stalled > 0) {
+        // the flagged cells, from their untouched inputs, with the FP64 LU
+        ReactParams Q = P;
+        Q.refine_stall = 0.0;
+        Q.retry_pass = 1;
+        if ((err = launch_rounds(h, Q, st, 8))) return err;
+      }
+    }
   }
   if (stats) {
     long long st_h[kStCount];
@@ -699,6 +726,7 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
     stats->ncfn = st_h[kStNcfn];
     stats->max_nfe = (int32_t)st_h[kStMaxNfe];
     stats->max_nst = (int32_t)st_h[kStMaxNst];
+    stats->n_fp64_retry = st_h[kStStall];
     if (stats->n_failed > 0) return set_err(B200CHEM_EINTEGRATE, "%lld cell(s) failed to integrate", stats->n_failed);
   }
   return 0;
@@ -1370,6 +1398,7 @@ extern "C" int b200chem_react_flat_noalloc(b200chem_handle h, double* rhoY, cons
     stats->ncfn = st_h[kStNcfn];
     stats->max_nfe = (int32_t)st_h[kStMaxNfe];
     stats->max_nst = (int32_t)st_h[kStMaxNst];
+    stats->n_fp64_retry = st_h[kStStall];
     if (time) *time += *dt_react;
     if (stats->n_failed > 0) return set_err(B200CHEM_EINTEGRATE, "%lld cell(s) failed to integrate", stats->n_failed);
     return 0;
@@ -1643,6 +1672,7 @@ int b200chem_destroy(b200chem_handle h) {
   staged_free(h->cboxes);
   staged_free(h->fboxes);
   if (h->d_zero_mask) cudaFree(h->d_zero_mask);
+  if (h->d_retry) cudaFree(h->d_retry);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->h_pcnt) cudaFreeHost(h->h_pcnt);
   if (h->cap_stream) cudaStreamDestroy(h->cap_stream);

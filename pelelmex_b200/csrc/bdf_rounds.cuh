@@ -483,10 +483,13 @@ __device__ __forceinline__ void g_apply_inverse(const LUT* A, const double (&dsc
 // step r = dl - (x - gamma_lu J x), x += A r; FP64 inverse: no refinement),
 // scaled by 2 / (1 + gamrat) when gamma has moved since the setup; then
 // acor += x.  Returns the WRMS norms of x (*del) and of the new acor (*anrm).
+// Internal status of a cell stopped for the FP64 retry (never reported).
+constexpr int kStatusRefineStall = -100;
+
 template <int n, int G, typename LUT>
 __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, const LUT* A, double rl1, double gamma,
                                          double gamma_lu, double gamrat, int gl, unsigned gm, double* del,
-                                         double* anrm) {
+                                         double* anrm, double stall_ratio, bool* stall) {
   constexpr int CPL = (n + G - 1) / G;
   double dl[CPL], x[CPL], dsc[CPL];
 #pragma unroll
@@ -515,8 +518,23 @@ __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, cons
 #pragma unroll
     for (int cc = 0; cc < CPL; ++cc) r[cc] = dl[cc] - (x[cc] - gamma_lu * r[cc]);
     g_apply_inverse<n, G, LUT>(A, dsc, r, gl, gm);
+    double r2 = 0.0, x2 = 0.0;
 #pragma unroll
-    for (int cc = 0; cc < CPL; ++cc) x[cc] += r[cc];
+    for (int cc = 0; cc < CPL; ++cc) {
+      const int i = gl + G * cc;
+      if (i < n) {
+        const double w = v.ewt(i);
+        r2 += (r[cc] * w) * (r[cc] * w);
+        x2 += (x[cc] * w) * (x[cc] * w);
+      }
+      x[cc] += r[cc];
+    }
+    // the refinement step must be small against the correction it refines
+    if (stall_ratio > 0.0) {
+      r2 = gsum<G>(r2, gm);
+      x2 = gsum<G>(x2, gm);
+      *stall = !(r2 <= stall_ratio * stall_ratio * x2);
+    }
   }
   const double sc = (gamrat != 1.0) ? 2.0 / (1.0 + gamrat) : 1.0;
   double s2 = 0.0, a2 = 0.0;
@@ -542,7 +560,8 @@ __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, cons
 // finished (kDone, *status set).
 template <int n, int G, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
-                                         const double* J, const LUT* A, int gl, unsigned gm, int* status) {
+                                         const double* J, const LUT* A, int gl, unsigned gm, int* status,
+                                         double stall_ratio = 0.0) {
   for (int guard = 0; guard < 256; ++guard) {
     switch (lab) {
       case kLAfterF0: {
@@ -702,7 +721,15 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       case kLNewtonIter: {
         c.cnt.nni++;
         double del, anrm;
-        g_newton<n, G, LUT>(v, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, gl, gm, &del, &anrm);
+        bool stall = false;
+        g_newton<n, G, LUT>(v, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, gl, gm, &del, &anrm, stall_ratio,
+                            &stall);
+        if (stall) {
+          // the FP32 inverse does not resolve this iteration matrix: the cell
+          // is left untouched for the pass with the FP64 LU
+          *status = kStatusRefineStall;
+          return kDone;
+        }
         if (c.mnewt > 0) c.crate = fmax(kCRDOWN * c.crate, del / c.delp);
         const double dcon = del * fmin(1.0, c.crate) / c.tq[4];
         if (dcon <= 1.0) {

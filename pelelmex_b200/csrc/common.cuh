@@ -49,7 +49,7 @@ cudaError_t react_force_launch(const ForceBoxDev* d_boxes, int nbox, long long t
 
 // stats slots in the scratch buffer (after the queue counter)
 enum { kStCells = 0, kStMasked, kStFailed, kStNst, kStNfe, kStNje, kStNlu, kStNetf, kStNcfn, kStMaxNfe,
-       kStMaxNst, kStCount };
+       kStMaxNst, kStStall, kStCount };
 
 struct ReactParams {
   DevMech mech;
@@ -64,6 +64,15 @@ struct ReactParams {
   unsigned long long* queue;
   long long* stats;
   int* status;
+  // round-based integrator, FP32 inverse: a Newton correction whose FP64
+  // refinement step is larger than refine_stall times the correction itself
+  // (the FP32 inverse does not resolve the iteration matrix) stops the cell
+  // untouched and flags it in retry[cell] for a pass with the FP64 LU
+  // (refine_stall <= 0: no check); retry_pass = 1 integrates only the
+  // flagged cells
+  double refine_stall;
+  int* retry;
+  int retry_pass;
 };
 
 __device__ __forceinline__ double* elem(const DevArr& a, int i, int j, int k) {

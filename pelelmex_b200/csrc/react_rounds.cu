@@ -336,7 +336,9 @@ __global__ void __launch_bounds__(128) rk_start(RoundsParams R) {
     const long long slot = base + threadIdx.x;
     const bool live = slot < R.nchunk;
     bool go = false, done = false, masked = false;
-    if (live) {
+    // the FP64 retry pass integrates only the cells the FP32 pass flagged
+    const bool skip = live && P.retry_pass && P.retry[R.chunk0 + slot] == 0;
+    if (live && !skip) {
       const long long cell = R.chunk0 + slot;
       const CellLoc L = locate(P, cell);
       const DevBox& bx = *L.bx;
@@ -466,7 +468,8 @@ __device__ __forceinline__ void ctrl_cell(const RoundsParams& R, bool live, int 
     if (after_rhs) c.cnt.nfe++;
     const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
     need = r_advance<n, G, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
-                                reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status);
+                                reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status,
+                                sizeof(LUT) == 4 ? P.refine_stall : 0.0);
     __syncwarp(gm);
     if (gl == 0) store_cell(c, rec);
     if (need == kDone) {
@@ -490,8 +493,14 @@ __device__ __forceinline__ void ctrl_cell(const RoundsParams& R, bool live, int 
         }
       }
       if (gl == 0) {
-        if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
-        if (P.status) P.status[cell] = status;
+        if (status == kStatusRefineStall) {
+          // untouched: no outputs, no status; the FP64 pass writes them
+          P.retry[cell] = 1;
+          if (P.stats) atomicAdd(reinterpret_cast<unsigned long long*>(P.stats + kStStall), 1ull);
+        } else {
+          if (bx.fc.p) *elem(bx.fc, L.i, L.j, L.k) = (double)c.cnt.nfe;
+          if (P.status) P.status[cell] = status;
+        }
       }
     }
   }
@@ -499,7 +508,7 @@ __device__ __forceinline__ void ctrl_cell(const RoundsParams& R, bool live, int 
   warp_append(lead && need == kNeedRhs, slot, R.list_out, R.cnt_out);
   warp_append(lead && (need == kNeedSetup || need == kNeedSetupJac), slot, R.list_setup, R.cnt_setup);
   warp_append(lead && need == kNeedSetupJac, slot, R.list_jac, R.cnt_jac);
-  warp_stats(P.stats, lead && need == kDone, status != 0, false, c.cnt);
+  warp_stats(P.stats, lead && need == kDone && status != kStatusRefineStall, status != 0, false, c.cnt);
 }
 
 // Resume the cells of list_in, G lanes per cell.  after_rhs: each consumes

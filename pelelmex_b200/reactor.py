@@ -107,7 +107,7 @@ class ReactorB200:
     KERNELS = {"auto": 0, "thread": 1, "group": 2, "rounds": 3}
 
     def __init__(self, mechanism=None, rtol: float = 1e-10, atol: float = 1e-10, max_order: int = 2,
-                 max_steps: int = 10000, lu_fp64: bool = False, warps_per_cta: int = 0, kernel: str = "auto",
+                 max_steps: int = 10000, lu_fp64: bool = False, refine_stall_ppm: int = 0, kernel: str = "auto",
                  setup_ratio: int = 0, ctas_per_sm: int = 0, group_lanes: int = 0):
         if mechanism is None:
             raise ValueError("a mechanism (name of a bundled file, path, or Mechanism) is required")
@@ -118,7 +118,7 @@ class ReactorB200:
         self.mech = mechanism
         self.flat = mechmod.flatten(mechanism)
         self.N = self.flat.n_species
-        self.opts = _lib.Opts(rtol, atol, max_order, max_steps, 2, 1 if lu_fp64 else 0, warps_per_cta, 0,
+        self.opts = _lib.Opts(rtol, atol, max_order, max_steps, 2, 1 if lu_fp64 else 0, refine_stall_ppm, 0,
                               self.KERNELS[kernel], setup_ratio, ctas_per_sm, group_lanes)
         self._h = None
         self._typ = None
@@ -134,7 +134,7 @@ class ReactorB200:
                    atol=float(params.get("ode.atol", 1e-10)), max_order=int(params.get("cvode.max_order", 2)),
                    max_steps=int(params.get("cvode.max_substeps", 10000)),
                    lu_fp64=bool(int(params.get("b200.lu_fp64", 0))),
-                   warps_per_cta=int(params.get("b200.warps_per_cta", 0)),
+                   refine_stall_ppm=int(params.get("b200.refine_stall_ppm", 0)),
                    kernel=params.get("b200.kernel", "auto"), setup_ratio=int(params.get("b200.setup_ratio", 0)),
                    ctas_per_sm=int(params.get("b200.ctas_per_sm", 0)),
                    group_lanes=int(params.get("b200.group_lanes", 0)))

@@ -117,3 +117,29 @@ def test_rounds_status_mask_and_bad_inputs(orc_cache):
     o = _oracle(orc_cache, "synth_h2_9", f3, max_steps=3)
     assert (g["status"] == -1).any()
     assert ((g["status"] == -1) == (o["status"] == -1)).mean() > 0.9
+
+
+def test_fp64_fallback_of_stalled_refinement(orc_cache):
+    """Per-cell FP64 fallback: a cell whose FP64 refinement step is not small
+    against its FP32-inverse Newton correction stops untouched and is
+    integrated again from its input with the FP64 LU in the same call.  A
+    stall bound of one part per million sends most cells through it: they are
+    counted once, succeed, and match the oracle at the parity tolerances; with
+    the check off no cell is retried."""
+    name = "synth_ch4_21"
+    mech = M.builtin(name)
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 4096, seed=44), dt=1e-5)
+    forced = run_gpu(name, f, kernel="rounds", refine_stall_ppm=1)
+    never = run_gpu(name, f, kernel="rounds", refine_stall_ppm=-1)
+    default = run_gpu(name, f, kernel="rounds")
+    retried = forced["stats"]["n_fp64_retry"]
+    print(f"{retried} of {f.ncells} cells through the FP64 fallback (default bound: "
+          f"{default['stats']['n_fp64_retry']})")
+    assert retried > f.ncells // 4
+    assert never["stats"]["n_fp64_retry"] == 0
+    assert (forced["status"] == 0).all()
+    st = forced["stats"]
+    assert st["n_cells"] == f.ncells and st["n_failed"] == 0
+    assert st["nfe"] == int(forced["fct"].sum())
+    o = _oracle(orc_cache, name, f)
+    compare(f, forced, o, "FP64 fallback forced")
