@@ -470,7 +470,9 @@ typedef struct b200chem_surrogate* b200chem_surrogate_handle;
 
 /* Loads an ensemble (the weights file above, from memory or from a path) to
  * the reactor's device, which must be current.  NULL on failure (message in
- * b200chem_last_error). */
+ * b200chem_last_error).  A surrogate owns its inference and fallback scratch
+ * (allocated on first use, grown as needed): calls with the same surrogate
+ * must not overlap in time. */
 b200chem_surrogate_handle b200chem_surrogate_load(b200chem_handle h, const void* data, size_t nbytes);
 b200chem_surrogate_handle b200chem_surrogate_load_file(b200chem_handle h, const char* path);
 /* The acceptance rule stored in the file. */

@@ -315,18 +315,19 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
         tgt[ne] = rhoH1;
         rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
         // weighted minimum-norm correction z' = z - W A^T (A W A^T)^-1 (A z - b)
-        // over the ne + 1 scaled rows A (zero rows are skipped).  Pass 0:
-        // W = max(|z_k|, 1e-10 rho).  Partial densities it leaves slightly
-        // negative are set to zero and frozen (W_k = 0) for pass 1, which
-        // restores the constraints exactly without moving them.
+        // over the ne + 1 scaled rows A (zero rows are skipped), with
+        // W = max(|z_k|, 1e-10 rho).  Partial densities a pass leaves
+        // slightly negative are set to zero and frozen (W_k = 0) for the
+        // next.  Three passes: each recomputes the constraint residuals, so
+        // the rounding of an ill-conditioned A W A^T and the clipped amounts
+        // are corrected again, down to round-off.
         const int nr = ne + 1;
         auto row = [&](int e, int k) -> double {
           return (e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k]) * rsc[e];
         };
-        bool frozen_any = false;
         unsigned long long frozen[(NS + 63) / 64] = {};
-        for (int pass = 0; pass < 2 && !reason; ++pass) {
-          if (pass == 1 && !frozen_any) break;
+        constexpr int kPasses = 3;
+        for (int pass = 0; pass < kPasses && !reason; ++pass) {
           double wk[NS];
 #pragma unroll
           for (int k = 0; k < NS; ++k)
@@ -380,10 +381,7 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
             if (z[k] < -P.o.tol_mass * rho1t) reason = kRejNegative;
             if (z[k] < 0.0) {
               z[k] = 0.0;
-              if (pass == 0) {
-                frozen[k >> 6] |= 1ull << (k & 63);
-                frozen_any = true;
-              }
+              frozen[k >> 6] |= 1ull << (k & 63);
             }
           }
         }
@@ -439,11 +437,324 @@ int launch_gate(const GateParams& P, int sm_count, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? 0 : B200CHEM_ECUDA;
 }
 
+// Lane-group form of the gate (G lanes per cell, component j of the cell on
+// lane j % G), used when the residual check is off: the same checks, in the
+// same order and with the same arithmetic per component, with the sums over
+// species as butterfly reductions inside the group (bitwise identical on
+// every lane, so every decision is uniform in the group) and the small
+// constraint system solved redundantly by every lane.  No per-thread arrays
+// of the cell's size, so no local memory.
+template <int G>
+__device__ __forceinline__ double grp_sum(double v, unsigned gm) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, G);
+  return v;
+}
+template <int G>
+__device__ __forceinline__ double grp_max(double v, unsigned gm) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(gm, v, o, G));
+  return v;
+}
+
+template <int NS, int G>
+__global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
+  constexpr int n = NS + 1;
+  constexpr int CPL = (n + G - 1) / G;
+  constexpr int kout = sg_out(NS);
+  __shared__ DevMech s_mech;
+  if (threadIdx.x == 0) s_mech = P.mech;
+  __syncthreads();
+  const DevMech& m = s_mech;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % G;
+  const unsigned gm = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane - gl));
+  const int per_block = blockDim.x / G;
+  for (long long base = (long long)blockIdx.x * per_block; base < P.nc; base += (long long)gridDim.x * per_block) {
+    const long long r = base + threadIdx.x / G;
+    const bool in = r < P.nc;
+    const long long c = P.c0 + r;
+    const bool masked = in && P.mask && P.mask[c] == 0;
+    int reason = kAccept;
+    if (in && !masked) {
+      // this lane's components: j = gl + G cc (0: T, k + 1: species k)
+      double y0[CPL], F[CPL], d[CPL], z[CPL], hk[CPL], a_row[CPL];
+      double rs = 0.0;
+#pragma unroll
+      for (int cc = 0; cc < CPL; ++cc) {
+        const int j = gl + G * cc;
+        y0[cc] = F[cc] = d[cc] = z[cc] = hk[cc] = 0.0;
+        if (j >= 1 && j < n) {
+          y0[cc] = P.rhoY[(long long)(j - 1) * P.ld + c];
+          F[cc] = P.fY[(long long)(j - 1) * P.ld + c];
+          rs += y0[cc];
+        } else if (j == 0) {
+          y0[cc] = P.T[c];
+          F[cc] = P.fH[c];
+        }
+      }
+      const double rho0 = grp_sum<G>(rs, gm);
+      // decoded changes: ensemble mean per component, extremes of dT
+      double tmin = 1e300, tmax = -1e300;
+      for (int mb = 0; mb < P.members; ++mb) {
+        const float* pr = P.pred + ((long long)mb * P.rows + r) * kout;
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int j = gl + G * cc;
+          if (j < n) {
+            const double u = (double)pr[j] * (double)P.ystd[j] + (double)P.ymean[j];
+            const double v = P.tscale[j] * sinh(u);
+            d[cc] += v;
+            if (j == 0) {
+              tmin = fmin(tmin, v);
+              tmax = fmax(tmax, v);
+            }
+          }
+        }
+      }
+      const double invM = 1.0 / P.members;
+#pragma unroll
+      for (int cc = 0; cc < CPL; ++cc) d[cc] *= invM;
+      const int src = lane - gl;  // the group's first lane holds T
+      const double dT = __shfl_sync(gm, d[0], src, 32);
+      const double T0 = __shfl_sync(gm, y0[0], src, 32);
+      const double FH = __shfl_sync(gm, F[0], src, 32);
+      tmin = __shfl_sync(gm, tmin, src, 32);
+      tmax = __shfl_sync(gm, tmax, src, 32);
+      const double T1 = T0 + dT;
+      const double bar = P.o.t_rel * T1;
+      const bool fin = rho0 > 0.0 && T0 > 0.0 && isfinite(dT) && T1 > 0.0;
+      if (!fin) reason = kRejNonfinite;
+      if (!reason && fmax(tmax - dT, dT - tmin) > P.o.spread * bar) reason = kRejSpread;
+      if (!reason && fabs(dT) > P.o.dT_cap * bar) reason = kRejCap;
+      // predicted partial densities and their target sum
+      double zs = 0.0, tsum = 0.0;
+      bool bad = false;
+#pragma unroll
+      for (int cc = 0; cc < CPL; ++cc) {
+        const int j = gl + G * cc;
+        if (j >= 1 && j < n) {
+          z[cc] = rho0 * (y0[cc] / rho0 + d[cc]) + P.dt * F[cc];
+          zs += z[cc];
+          tsum += y0[cc] + P.dt * F[cc];
+          bad |= !isfinite(z[cc]);
+        }
+      }
+      const double rho1t = grp_sum<G>(tsum, gm);
+      zs = grp_sum<G>(zs, gm);
+      bad = grp_max<G>(bad ? 1.0 : 0.0, gm) > 0.0;
+      if (!reason && bad) reason = kRejNonfinite;
+      if (!reason && !(fabs(zs - rho1t) <= P.o.tol_mass * rho1t)) reason = kRejMass;
+      const int ne = P.ne < kMaxElem ? P.ne : kMaxElem;
+      double tgt[kMaxElem + 1], rsc[kMaxElem + 1];
+      const double rhoH1 = P.rhoH[c] + P.dt * FH;
+      if (!reason) {
+        double tot = 0.0, worst = 0.0;
+        for (int e = 0; e < ne; ++e) {
+          double ct = 0.0, cz = 0.0, mx = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int j = gl + G * cc;
+            if (j >= 1 && j < n) {
+              const double a = __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1));
+              ct += a * (y0[cc] + P.dt * F[cc]);
+              cz += a * z[cc];
+              mx = fmax(mx, fabs(a));
+            }
+          }
+          ct = grp_sum<G>(ct, gm);
+          cz = grp_sum<G>(cz, gm);
+          mx = grp_max<G>(mx, gm);
+          tgt[e] = ct;
+          rsc[e] = mx > 0.0 ? 1.0 / mx : 0.0;
+          tot += ct;
+          worst = fmax(worst, fabs(cz - ct));
+        }
+        if (!(worst <= P.o.tol_elem * tot)) reason = kRejElem;
+      }
+      if (!reason) {
+        // energy consistency of the raw prediction: T(h1, Y(z)) against T1
+        double zsum = 0.0;
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int j = gl + G * cc;
+          if (j >= 1 && j < n) zsum += fmax(z[cc], 0.0);
+        }
+        zsum = grp_sum<G>(zsum, gm);
+        const double h1 = rhoH1 / zsum;
+        double Th = T1;
+        bool conv = false;
+        for (int it = 0; it < 50 && Th > 0.0 && !conv; ++it) {
+          const double lnT = log(Th);
+          double hs = 0.0, cs = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int j = gl + G * cc;
+            if (j >= 1 && j < n) {
+              double cpR, hRT, sR, dcpR;
+              nasa7(m, j - 1, Th, lnT, cpR, hRT, sR, dcpR);
+              const double w = fmax(z[cc], 0.0) / zsum * __ldg(m.inv_mw + (j - 1)) * kRu;
+              hs += w * hRT * Th;
+              cs += w * cpR;
+            }
+          }
+          hs = grp_sum<G>(hs, gm);
+          cs = grp_sum<G>(cs, gm);
+          const double dTn = (h1 - hs) / cs;
+          Th += dTn;
+          conv = fabs(dTn) <= 1e-10 * Th;
+        }
+        if (!conv || !(fabs(Th - T1) <= P.o.gap * bar)) reason = kRejEnergy;
+      }
+      if (!reason) {
+        // species enthalpies at T1: the energy row
+        const double lnT1 = log(T1);
+        double mx = 0.0;
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int j = gl + G * cc;
+          if (j >= 1 && j < n) {
+            double cpR, hRT, sR, dcpR;
+            nasa7(m, j - 1, T1, lnT1, cpR, hRT, sR, dcpR);
+            hk[cc] = hRT * kRu * T1 * __ldg(m.inv_mw + (j - 1));
+            mx = fmax(mx, fabs(hk[cc]));
+          }
+        }
+        mx = grp_max<G>(mx, gm);
+        tgt[ne] = rhoH1;
+        rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
+        // weighted minimum-norm correction z' = z - W A^T (A W A^T)^-1 (A z - b)
+        // over the ne + 1 scaled rows A, three passes (see hy_gate)
+        const int nr = ne + 1;
+        unsigned frozen = 0;  // bit cc: this lane's component cc is frozen at zero
+        for (int pass = 0; pass < 3 && !reason; ++pass) {
+          double Gm[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
+          for (int e = 0; e < nr; ++e) {
+#pragma unroll
+            for (int cc = 0; cc < CPL; ++cc) {
+              const int j = gl + G * cc;
+              a_row[cc] = 0.0;
+              if (j >= 1 && j < n)
+                a_row[cc] = (e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) *
+                            rsc[e];
+            }
+            double az = 0.0;
+#pragma unroll
+            for (int cc = 0; cc < CPL; ++cc) az += a_row[cc] * z[cc];
+            lam[e] = grp_sum<G>(az, gm) - tgt[e] * rsc[e];
+            for (int f = 0; f <= e; ++f) {
+              double g = 0.0;
+#pragma unroll
+              for (int cc = 0; cc < CPL; ++cc) {
+                const int j = gl + G * cc;
+                if (j >= 1 && j < n && !((frozen >> cc) & 1u)) {
+                  const double af = (f < ne ? __ldg(P.elem + f * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) *
+                                    rsc[f];
+                  g += a_row[cc] * af * fmax(fabs(z[cc]), 1e-10 * rho0);
+                }
+              }
+              Gm[e][f] = Gm[f][e] = grp_sum<G>(g, gm);
+            }
+          }
+          // Gauss-Jordan with partial pivoting (singular pivots: row skipped)
+          for (int col = 0; col < nr; ++col) {
+            int piv = col;
+            for (int w = col + 1; w < nr; ++w)
+              if (fabs(Gm[w][col]) > fabs(Gm[piv][col])) piv = w;
+            if (!(fabs(Gm[piv][col]) > 1e-300)) continue;
+            if (piv != col) {
+              for (int w = 0; w < nr; ++w) {
+                const double t = Gm[col][w];
+                Gm[col][w] = Gm[piv][w];
+                Gm[piv][w] = t;
+              }
+              const double t = lam[col];
+              lam[col] = lam[piv];
+              lam[piv] = t;
+            }
+            const double inv = 1.0 / Gm[col][col];
+            for (int w = 0; w < nr; ++w) {
+              if (w == col) continue;
+              const double f = Gm[w][col] * inv;
+              if (f == 0.0) continue;
+              for (int v = col; v < nr; ++v) Gm[w][v] -= f * Gm[col][v];
+              lam[w] -= f * lam[col];
+            }
+          }
+          for (int e = 0; e < nr; ++e) lam[e] = (fabs(Gm[e][e]) > 1e-300) ? lam[e] / Gm[e][e] : 0.0;
+          bool neg = false;
+#pragma unroll
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int j = gl + G * cc;
+            if (j >= 1 && j < n && !((frozen >> cc) & 1u)) {
+              double corr = 0.0;
+              for (int e = 0; e < nr; ++e)
+                corr += (e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) * rsc[e] *
+                        lam[e];
+              z[cc] -= fmax(fabs(z[cc]), 1e-10 * rho0) * corr;
+              if (z[cc] < -P.o.tol_mass * rho1t) neg = true;
+              if (z[cc] < 0.0) {
+                z[cc] = 0.0;
+                frozen |= 1u << cc;
+              }
+            }
+          }
+          if (grp_max<G>(neg ? 1.0 : 0.0, gm) > 0.0) reason = kRejNegative;
+        }
+      }
+      if (!reason) {
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int j = gl + G * cc;
+          if (j >= 1 && j < n) P.rhoY[(long long)(j - 1) * P.ld + c] = z[cc];
+        }
+        if (gl == 0) {
+          P.T[c] = T1;
+          P.rhoH[c] = rhoH1;
+          if (P.fct) P.fct[c] = 0.0;
+          if (P.status) P.status[c] = B200CHEM_CELL_OK;
+        }
+      }
+    } else if (masked && gl == 0) {
+      if (P.fct) P.fct[c] = 0.0;
+      if (P.status) P.status[c] = B200CHEM_CELL_MASKED;
+    }
+    // group leaders: warp-aggregated append of the rejected cells and counts
+    const bool lead = in && !masked && gl == 0;
+    const bool rej = lead && reason != kAccept;
+    const unsigned bal = __ballot_sync(0xffffffffu, rej);
+    if (bal) {
+      int basei = 0;
+      if (lane == 0) basei = atomicAdd(P.rej_count, __popc(bal));
+      basei = __shfl_sync(0xffffffffu, basei, 0);
+      if (rej) P.rej_list[basei + __popc(bal & ((1u << lane) - 1u))] = (int)c;
+    }
+#pragma unroll
+    for (int q = 0; q < kReasons; ++q) {
+      const unsigned b = __ballot_sync(0xffffffffu, lead && reason == q);
+      if (b && lane == 0) atomicAdd(P.reasons + q, (unsigned long long)__popc(b));
+    }
+  }
+}
+
+template <int NS>
+int launch_gate_grp(const GateParams& P, int sm_count, cudaStream_t st) {
+  constexpr int G = NS + 1 <= 32 ? 8 : 16;
+  const int per_block = 128 / G;
+  const long long need = (P.nc + per_block - 1) / per_block;
+  const long long cap = 32LL * sm_count;
+  hy_gate_grp<NS, G><<<(unsigned)(need < cap ? need : cap), 128, 0, st>>>(P);
+  return cudaGetLastError() == cudaSuccess ? 0 : B200CHEM_ECUDA;
+}
+
+// The lane-group gate unless the residual check (a per-cell right-hand
+// side) is on.
 int gate_for(int N, const GateParams& P, int sm_count, cudaStream_t st) {
+  const bool grp = !(P.o.resid > 0.0);
   switch (N) {
-    case 9: return launch_gate<9>(P, sm_count, st);
-    case 21: return launch_gate<21>(P, sm_count, st);
-    case 53: return launch_gate<53>(P, sm_count, st);
+    case 9: return grp ? launch_gate_grp<9>(P, sm_count, st) : launch_gate<9>(P, sm_count, st);
+    case 21: return grp ? launch_gate_grp<21>(P, sm_count, st) : launch_gate<21>(P, sm_count, st);
+    case 53: return grp ? launch_gate_grp<53>(P, sm_count, st) : launch_gate<53>(P, sm_count, st);
     default: return B200CHEM_EINVAL;
   }
 }
