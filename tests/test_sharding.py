@@ -92,3 +92,47 @@ def test_rebalance_follows_the_threshold_rule():
     assert np.array_equal(owner2, balanced)  # no gain above the threshold: keep
     # the cost of a box is the sum of its cells' fctCount
     assert np.allclose(sharding.box_costs([np.ones(8) * 3, np.arange(4)]), [24.0, 6.0])
+
+
+def _leaver(rank, world, port, q):
+    """Rank 1 leaves between steps (after the first step's reduction, with
+    nothing in flight); rank 0's next step-time reduction must end with an
+    error within the process group's short timeout, not hang."""
+    import datetime
+    import time
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    ms = sharding.step_time_max(1.0 + rank)
+    if rank == 1:
+        q.put((rank, ms, "left", 0.0))
+        q.close()
+        q.join_thread()
+        os._exit(0)  # leaves without tearing the group down, as a crashed rank would
+    t0 = time.time()
+    try:
+        sharding.step_time_max(2.0)
+        q.put((rank, ms, "no error", time.time() - t0))
+    except Exception as e:  # noqa: BLE001 - the failure surfaces as an error of the collective
+        q.put((rank, ms, type(e).__name__, time.time() - t0))
+    q.close()
+    q.join_thread()
+    os._exit(0)
+
+
+def test_rank_leaving_between_steps_fails_the_next_reduction():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_leaver, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict((r[0], r) for r in (q.get(timeout=120) for _ in range(world)))
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert out[1][2] == "left" and out[0][1] == 2.0 and out[1][1] == 2.0
+    # rank 0: the reduction of the second step raised instead of hanging
+    assert out[0][2] != "no error"
+    assert out[0][3] < 60.0
