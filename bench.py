@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--cells", type=int, default=0,
                    help="react only this many seeded random cells of the field (small profiling cases)")
     p.add_argument("--no-hybrid", action="store_true", help="plain BDF only (no surrogate arm)")
+    p.add_argument("--no-c12", action="store_true", help="skip the dodecane box-list block of the headline line")
     p.add_argument("--no-autotune", action="store_true", help="default launch shape (no autotuner pass)")
     p.add_argument("--tune-cells", type=int, default=262144, help="cells of the autotuner's sample")
     return p.parse_args()
@@ -596,6 +597,10 @@ def run_b200(args, rank, world, local_rank, field):
         mlp_flops = 2.0 * ((N + 2 + 15) // 16 * 16 * 256 + 2 * 256 * 256 + 256 * ((N + 1 + 15) // 16 * 16))
         hybrid["mlp_flops_per_cell_per_member"] = mlp_flops
 
+    c12 = None
+    if not args.no_c12 and not args.cells:
+        c12 = c12_boxes_block(args, dev, stream, barrier, world, rank)
+
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu:
         rate, n, threads, el = cpu_sample_run(mech, args, args.cpu_seconds)
@@ -613,13 +618,88 @@ def run_b200(args, rank, world, local_rank, field):
               "integrator": HYBRID_INTEGRATOR if use_hybrid else GPU_INTEGRATOR, "launch_tuning": launch_tuning,
               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
               "gpu_launches": launches if path != "hybrid" else hybrid["gpu_launches"], "clocks": clk.summary(),
-              "plain_gpu_bdf": plain, "hybrid": hybrid, "dt_blocks": blocks,
+              "plain_gpu_bdf": plain, "hybrid": hybrid, "dt_blocks": blocks, "c12_boxes": c12,
               "counters": {k: int(v) for k, v in counters.items()}})
     r.close()
 
 
 # ------------------------------------------------------ dodecane workloads
 C12 = "synth_c12_53"
+
+
+def _gen_c12_box(a):
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    dt, b = a
+    return workloads.c12_boxes(mechmod.builtin(C12), dt=dt, only={b})[0]
+
+
+def c12_box_list(dt, nbox=40):
+    """The dodecane AMR-like box list, one box per task of a pool of host
+    processes (each box depends only on the seed and its index)."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(nbox, os.cpu_count() or 1)) as pool:
+        return pool.map(_gen_c12_box, [(dt, b) for b in range(nbox)])
+
+
+def c12_boxes_block(args, dev, stream, barrier, world, rank=0):
+    """The C3 workload beside the headline: the 40-box dodecane list in one
+    react launch per step (2 warm-up, 3 timed steps, CUDA events), and the
+    GPU result of 64 seeded cells per box against the CPU oracle (rtol 1e-8 /
+    atol 1e-12) and its tight solve (rtol 1e-12 / atol 1e-20)."""
+    import torch
+    from oracle import oracle as orc
+    from pelelmex_b200 import mechanism as mechmod, workloads
+    from pelelmex_b200.reactor import Box, ReactorB200
+    mech = mechmod.builtin(C12)
+    N = mech.n_species
+    boxes = c12_box_list(1e-6)
+    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    work, pristine, items = [], [], []
+    for lo, e, f in boxes:
+        w = {k: torch.tensor(getattr(f, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
+        w["fct"] = torch.zeros(f.ncells, dtype=torch.float64, device=dev)
+        work.append(w)
+        pristine.append({k: w[k].clone() for k in ("rhoY", "T", "rhoH")})
+        v = lambda t, c: t.view(c, e, e, e)  # noqa: E731
+        items.append((Box(lo, (lo[0] + e - 1, e - 1, e - 1)), v(w["rhoY"], N), v(w["frhoY"], N), v(w["T"], 1),
+                      v(w["rhoH"], 1), v(w["frhoH"], 1), v(w["fct"], 1), None))
+    total = sum(f.ncells for _, _, f in boxes)
+
+    def restore():
+        for w, p in zip(work, pristine):
+            for k in p:
+                w[k].copy_(p[k])
+    step_ms = time_steps(lambda: r.react_boxes(items, 1e-6), restore, 3, 2, stream, barrier)
+    ms = sharding.step_time_max(sum(step_ms) / len(step_ms), dev)
+    del work, pristine, items
+    out = {"workload": "c12_boxes: 40 dodecane boxes (edges 16/32/64, half cold 300-600 K, half igniting "
+                       "900-1400 K, phi 0.5-2), synth_c12_53, dt_react 1e-6 s, one react launch per box list",
+           "cells": total, "value": world * total / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": 3,
+           "step_ms": step_ms}
+    if rank != 0 or args.no_cpu:
+        r.close()
+        return out
+    # accuracy on 64 seeded cells per box
+    sub = workloads.c12_boxes(mech, dt=1e-6, box_cells=64)
+    cat = lambda key, ax: np.ascontiguousarray(np.concatenate([getattr(f, key) for _, _, f in sub], axis=ax))  # noqa
+    rY0, T0, rH0, fY, fH = cat("rhoY", 1), cat("T", 0), cat("rhoH", 0), cat("frhoY", 1), cat("frhoH", 0)
+    g = [torch.tensor(a, device=dev) for a in (rY0, T0, rH0, fY, fH)]
+    r.react_flat(g[0], g[3], g[1], g[2], g[4], dt_react=1e-6)
+    gT, gY = g[1].cpu().numpy(), g[0].cpu().numpy()
+    r.close()
+    o = orc.Oracle(mechmod.flatten(mech))
+    kw = dict(max_order=QMAX, max_steps=100000, nthreads=orc.max_threads())
+    ref = o.react(rY0, fY, T0, rH0, fH, 1e-6, rtol=RTOL, atol=ATOL, **kw)
+    tight = o.react(rY0, fY, T0, rH0, fH, 1e-6, **TIGHT, **kw)
+    rho = rY0.sum(axis=0)
+
+    def err(T, Y, RT, RY):
+        return {"max_rel_T": float(np.max(np.abs(T - RT) / RT)),
+                "max_abs_Y": float(np.max(np.abs(Y - RY).max(axis=0) / rho))}
+    out["sample"] = {"cells": int(T0.size), "gpu_vs_oracle": err(gT, gY, ref["T"], ref["rhoY"]),
+                     "gpu_vs_oracle_tight": err(gT, gY, tight["T"], tight["rhoY"]),
+                     "oracle_vs_oracle_tight": err(ref["T"], ref["rhoY"], tight["T"], tight["rhoY"])}
+    return out
 
 
 def _gen_c12_chunk(a):
@@ -697,7 +777,7 @@ def run_dodecane(args, rank, world, local_rank):
     mech = mechmod.builtin(C12)
     N = mech.n_species
     if args.workload == "c12_boxes":
-        boxes = workloads.c12_boxes(mech, dt=args.dt)
+        boxes = c12_box_list(args.dt)
         mine = sharding.shard_boxes(boxes, rank, world)
         total = sum(f.ncells for _, _, f in boxes)
         wl = (f"c12_boxes: {len(boxes)} dodecane boxes (edges 16/32/64, half cold 300-600 K, half igniting "

@@ -427,8 +427,11 @@ int b200chem_mlp_adam(float* p, const float* g, float* m, float* v, int rows, in
  * No reference counterpart: the surrogate-first react.  An ensemble of
  * networks predicts every cell's change over dt_react; a prediction is
  * accepted only when the acceptance rule below holds, and the accepted state
- * is corrected to conserve the element totals and the energy exactly; the
- * other cells are integrated by the BDF of b200chem_react_flat.
+ * is corrected to conserve the element totals and the energy exactly (a
+ * state the correction leaves more than 1e-13 off a constraint, relative to
+ * the atom content or to sum_k |h_k rhoY_k|, is rejected and counted in
+ * rejected_elements); the other cells are integrated by the BDF of
+ * b200chem_react_flat.
  *
  * Weights file (b200chem_surrogate_load), little endian:
  *   header (header_bytes, >= 128):

@@ -1476,7 +1476,7 @@ int tune_header(b200chem_handle h, TuneHeader* t) {
   t->digest = h->digest;
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, h->device));
-  snprintf(t->gpu, sizeof(t->gpu), "%s", prop.name);
+  strncpy(t->gpu, prop.name, sizeof(t->gpu) - 1);  // the name, cut to 63 bytes
   t->sm_count = h->sm_count;
   return 0;
 }

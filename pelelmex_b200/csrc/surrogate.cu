@@ -140,6 +140,13 @@ enum GateReason : int {
   kReasons = 9
 };
 
+// projection passes of the gate, and the relative residual every constraint
+// of an accepted cell must meet afterwards (elements: relative to the total
+// atom content; energy: relative to sum_k |h_k| z_k)
+constexpr int kMinPasses = 3;
+constexpr int kMaxPasses = 6;
+constexpr double kConsTol = 1e-13;
+
 struct GateParams {
   DevMech mech;
   double* rhoY;  // [N][ld] in/out
@@ -318,16 +325,19 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
         // over the ne + 1 scaled rows A (zero rows are skipped), with
         // W = max(|z_k|, 1e-10 rho).  Partial densities a pass leaves
         // slightly negative are set to zero and frozen (W_k = 0) for the
-        // next.  Three passes: each recomputes the constraint residuals, so
-        // the rounding of an ill-conditioned A W A^T and the clipped amounts
-        // are corrected again, down to round-off.
+        // next.  Each pass recomputes the constraint residuals, so the
+        // rounding of an ill-conditioned A W A^T and the clipped amounts are
+        // corrected again: at least kMinPasses passes, and more while the
+        // last one clipped (a cell still clipping after kMaxPasses is
+        // rejected).
         const int nr = ne + 1;
         auto row = [&](int e, int k) -> double {
           return (e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k]) * rsc[e];
         };
         unsigned long long frozen[(NS + 63) / 64] = {};
-        constexpr int kPasses = 3;
-        for (int pass = 0; pass < kPasses && !reason; ++pass) {
+        bool clipped = true;
+        for (int pass = 0; pass < kMaxPasses && !reason && (pass < kMinPasses || clipped); ++pass) {
+          clipped = false;
           double wk[NS];
 #pragma unroll
           for (int k = 0; k < NS; ++k)
@@ -382,8 +392,24 @@ __global__ void __launch_bounds__(kSgBlock) hy_gate(GateParams P) {
             if (z[k] < 0.0) {
               z[k] = 0.0;
               frozen[k >> 6] |= 1ull << (k & 63);
+              clipped = true;
             }
           }
+        }
+        if (!reason && clipped) reason = kRejNegative;
+        // every constraint met to round-off, or the cell goes to the BDF:
+        // the elements relative to the total atom content, the energy
+        // relative to sum_k |h_k| z_k
+        double tot = 0.0;
+        for (int e = 0; e < ne; ++e) tot += tgt[e];
+        for (int e = 0; e < nr && !reason; ++e) {
+          double az = 0.0, sc = 0.0;
+          for (int k = 0; k < NS; ++k) {
+            const double a = e < ne ? __ldg(P.elem + e * NS + k) * __ldg(m.inv_mw + k) : hk[k];
+            az += a * z[k];
+            sc += fabs(a) * z[k];
+          }
+          if (!(fabs(az - tgt[e]) <= kConsTol * (e < ne ? tot : sc))) reason = kRejElem;
         }
       }
       if (!reason && P.o.resid > 0.0) {
@@ -624,10 +650,11 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
         tgt[ne] = rhoH1;
         rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
         // weighted minimum-norm correction z' = z - W A^T (A W A^T)^-1 (A z - b)
-        // over the ne + 1 scaled rows A, three passes (see hy_gate)
+        // over the ne + 1 scaled rows A, the passes of hy_gate
         const int nr = ne + 1;
         unsigned frozen = 0;  // bit cc: this lane's component cc is frozen at zero
-        for (int pass = 0; pass < 3 && !reason; ++pass) {
+        bool clipped = true;
+        for (int pass = 0; pass < kMaxPasses && !reason && (pass < kMinPasses || clipped); ++pass) {
           double Gm[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
           for (int e = 0; e < nr; ++e) {
 #pragma unroll
@@ -682,7 +709,7 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
             }
           }
           for (int e = 0; e < nr; ++e) lam[e] = (fabs(Gm[e][e]) > 1e-300) ? lam[e] / Gm[e][e] : 0.0;
-          bool neg = false;
+          bool neg = false, clip = false;
 #pragma unroll
           for (int cc = 0; cc < CPL; ++cc) {
             const int j = gl + G * cc;
@@ -696,10 +723,32 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
               if (z[cc] < 0.0) {
                 z[cc] = 0.0;
                 frozen |= 1u << cc;
+                clip = true;
               }
             }
           }
           if (grp_max<G>(neg ? 1.0 : 0.0, gm) > 0.0) reason = kRejNegative;
+          clipped = grp_max<G>(clip ? 1.0 : 0.0, gm) > 0.0;
+        }
+        if (!reason && clipped) reason = kRejNegative;
+        // every constraint met to round-off, or the cell goes to the BDF
+        // (the scales of hy_gate)
+        double tot = 0.0;
+        for (int e = 0; e < ne; ++e) tot += tgt[e];
+        for (int e = 0; e < nr && !reason; ++e) {
+          double az = 0.0, sc = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int j = gl + G * cc;
+            if (j >= 1 && j < n) {
+              const double a = e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc];
+              az += a * z[cc];
+              sc += fabs(a) * z[cc];
+            }
+          }
+          az = grp_sum<G>(az, gm);
+          sc = grp_sum<G>(sc, gm);
+          if (!(fabs(az - tgt[e]) <= kConsTol * (e < ne ? tot : sc))) reason = kRejElem;
         }
       }
       if (!reason) {

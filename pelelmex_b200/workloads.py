@@ -244,19 +244,25 @@ def _c12_products(mech, Z):
     return mechmod.mole_to_mass(mech, X / X.sum(axis=1, keepdims=True))
 
 
-def c12_boxes(mech, seed: int = 3, dt: float = 1e-6, nbox: int = 40, edges=(16, 32, 64), box_cells=None):
+def c12_boxes(mech, seed: int = 3, dt: float = 1e-6, nbox: int = 40, edges=(16, 32, 64), box_cells=None,
+              only=None):
     """AMR-like dodecane box list: `nbox` cubic boxes with edges drawn from
     `edges`; the first half cold and inert (T ~ U[300, 600] K), the second
     half igniting (T ~ U[900, 1400] K); per cell phi ~ U[0.5, 2]
     (n-C12H26/air), +-2% noise on Y.  Returns [(lo, edge, Field)]; lo places
     the boxes side by side along x.  box_cells (optional) caps the cells
-    generated per box (a seeded subset, for parity samples)."""
+    generated per box (a seeded subset, for parity samples); `only`
+    (optional) generates just those box indices (each box depends only on
+    the seed and its index)."""
     out = []
     bidx = np.arange(nbox, dtype=np.int64)
     pick = np.minimum((uniform(seed, 0, bidx) * len(edges)).astype(np.int64), len(edges) - 1)
     x0 = 0
     for b in range(nbox):
         e = int(edges[pick[b]])
+        if only is not None and b not in only:
+            x0 += e
+            continue
         shape = (e, e, e)
         c = _cells(shape, None)
         if box_cells is not None and box_cells < c.size:
