@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--no-hybrid", action="store_true", help="plain BDF only (no surrogate arm)")
     p.add_argument("--no-c12", action="store_true", help="skip the dodecane box-list block of the headline line")
     p.add_argument("--no-autotune", action="store_true", help="default launch shape (no autotuner pass)")
+    p.add_argument("--refine-keep-ppm", type=int, default=0,
+                   help="> 0: FP32 solve accuracy (ppm) below which a Newton correction skips the FP64 refinement "
+                        "(0: refine every correction, the default)")
     p.add_argument("--tune-cells", type=int, default=262144, help="cells of the autotuner's sample")
     return p.parse_args()
 
@@ -363,7 +366,8 @@ def run_b200(args, rank, world, local_rank, field):
     N = mech.n_species
     cfg = workload_config(args)
 
-    r = ReactorB200(MECH, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    r = ReactorB200(MECH, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS,
+                    refine_keep_ppm=args.refine_keep_ppm).init()
     base = {k: torch.tensor(getattr(field, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
     rY, T, rH = (torch.empty_like(base[k]) for k in ("rhoY", "T", "rhoH"))
     fct = torch.zeros(nc, dtype=torch.float64, device=dev)
@@ -653,7 +657,8 @@ def c12_boxes_block(args, dev, stream, barrier, world, rank=0):
     mech = mechmod.builtin(C12)
     N = mech.n_species
     boxes = c12_box_list(1e-6)
-    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS,
+                    refine_keep_ppm=args.refine_keep_ppm).init()
     work, pristine, items = [], [], []
     for lo, e, f in boxes:
         w = {k: torch.tensor(getattr(f, k), device=dev) for k in ("rhoY", "T", "rhoH", "frhoY", "frhoH")}
@@ -813,7 +818,8 @@ def run_dodecane(args, rank, world, local_rank):
     props = torch.cuda.get_device_properties(dev)
     bus = getattr(props, "pci_bus_id", None)
     bus_id = f"{props.pci_domain_id:08x}:{bus:02x}:{props.pci_device_id:02x}.0" if bus is not None else None
-    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS).init()
+    r = ReactorB200(C12, rtol=RTOL, atol=ATOL, max_order=QMAX, max_steps=MAXSTEPS,
+                    refine_keep_ppm=args.refine_keep_ppm).init()
     stream = torch.cuda.current_stream(dev)
     # device state: working arrays plus pristine copies to restore between steps
     work, pristine = [], []

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define B200CHEM_VERSION 2
+#define B200CHEM_VERSION 3
 
 /* ---------------------------------------------------------------- errors */
 #define B200CHEM_OK 0
@@ -118,6 +118,21 @@ typedef struct b200chem_opts {
                             keeps the per-cell scratch in L2                  */
   int32_t group_lanes;   /* group integrator: lanes per cell, 8, 16 or 32
                             (0 = default for the mechanism size)              */
+  int32_t refine_keep_ppm; /* round-based integrator with the FP32 inverse,
+                            > 0: the first Newton correction after each setup
+                            is refined in FP64, which measures how accurate
+                            the FP32 solve is for that matrix (WRMS of the
+                            refinement step over the correction); the later
+                            corrections with the same matrix skip the
+                            refinement (and the Jacobian it reads) while that
+                            measure is at most this many parts per million.
+                            Faster (flame_ch4 128^3: 1.2x), but the unrefined
+                            corrections (~5e-8 relative) flip some step
+                            decisions against an FP64 solve: a few cells in
+                            10^4 then differ from the dense-direct result by
+                            more than 1e-8 in Y.  0 (default) or negative:
+                            refine every correction                           */
+  int32_t reserved;      /* 0                                                 */
 } b200chem_opts;
 
 /* ---------------------------------------------------------- Array4 views

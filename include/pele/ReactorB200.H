@@ -74,6 +74,8 @@ public:
     pc.query("max_substeps", o.max_steps);
     pb.query("lu_fp64", o.lu_fp64);
     pb.query("kernel", o.kernel);
+    pb.query("refine_stall_ppm", o.refine_stall_ppm);
+    pb.query("refine_keep_ppm", o.refine_keep_ppm);
     o.reactor_type = reactor_type;  // 2: HP
     const b200chem_mech_desc d = b200chem_make_mech_desc();
     h_ = b200chem_create(&d, &o);

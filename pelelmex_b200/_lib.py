@@ -21,7 +21,7 @@ class Opts(ctypes.Structure):
                 ("max_steps", ctypes.c_int32), ("reactor_type", ctypes.c_int32), ("lu_fp64", ctypes.c_int32),
                 ("refine_stall_ppm", ctypes.c_int32), ("verbose", ctypes.c_int32), ("kernel", ctypes.c_int32),
                 ("setup_ratio", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
-                ("group_lanes", ctypes.c_int32)]
+                ("group_lanes", ctypes.c_int32), ("refine_keep_ppm", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class Array4(ctypes.Structure):

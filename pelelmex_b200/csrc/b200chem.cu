@@ -676,6 +676,7 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
   P.stats = reinterpret_cast<long long*>(h->d_scratch + 1);
   P.status = cell_status;
   P.refine_stall = 0.0;
+  P.refine_keep = 0.0;
   P.retry = nullptr;
   P.retry_pass = 0;
   if (h->opts.kernel == 1 && !tpc_supported(h->N))
@@ -685,6 +686,8 @@ int do_react(b200chem_reactor* h, const std::vector<DevBox>& boxes, long long to
     // else the group integrator (any species count)
     const int k = (h->opts.kernel == 0) ? (rounds_supported(h->N) ? 3 : 2) : h->opts.kernel;
     const int ppm = h->opts.refine_stall_ppm;
+    const int keep = h->opts.refine_keep_ppm;
+    if (k == 3 && !h->opts.lu_fp64 && keep > 0) P.refine_keep = keep * 1e-6;
     if (k == 3 && !h->opts.lu_fp64 && ppm >= 0) {
       // per-cell FP64 fallback: flags of the cells whose refined FP32 solve stalls
       P.refine_stall = (ppm == 0 ? 250000 : ppm) * 1e-6;

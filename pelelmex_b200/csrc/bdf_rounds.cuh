@@ -56,7 +56,9 @@ struct alignas(16) RCell {
   int q, qprime, L, qwait, nstlp, nstlj, jcur, ncf, nef, nflag, convfail, callSetup, jbad, mnewt, attempt;
   int count1, hnewOK, nstloc, qmax, max_steps, setup_conv, label, setup_ier;
   CellCounters cnt;
-  int pad_[2];
+  float refine_ratio;  // WRMS of the last FP64 refinement step over its correction (kRefineUnknown: none since
+                       // the last setup)
+  int pad_;
 };
 static_assert(sizeof(RCell) % 16 == 0, "RCell moves as 16-byte vectors");
 
@@ -113,7 +115,7 @@ __device__ __forceinline__ unsigned char* rec_of(const RState& S, long long slot
   X(saved_tq5) X(gamma_lu) X(dt) X(saved_t) X(delp) X(hg) X(hub) X(hlb) X(q) X(qprime) X(L) X(qwait)      \
   X(nstlp) X(nstlj) X(jcur) X(ncf) X(nef) X(nflag) X(convfail) X(callSetup) X(jbad) X(mnewt) X(attempt)    \
   X(count1) X(hnewOK) X(nstloc) X(qmax) X(max_steps) X(setup_conv) X(label) X(setup_ier) X(cnt.nst)       \
-  X(cnt.nfe) X(cnt.nje) X(cnt.nlu) X(cnt.netf) X(cnt.ncfn) X(cnt.nni)
+  X(cnt.nfe) X(cnt.nje) X(cnt.nlu) X(cnt.netf) X(cnt.ncfn) X(cnt.nni) X(refine_ratio)
 
 __device__ __forceinline__ void load_cell(RCell& c, const unsigned char* rec) {
   const RCell* g = reinterpret_cast<const RCell*>(rec);
@@ -479,17 +481,21 @@ __device__ __forceinline__ void g_apply_inverse(const LUT* A, const double (&dsc
 }
 
 // One Newton correction: x = (I - gamma_lu J)^-1 dl with
-// dl = -(rl1 zn[1] + acor - gamma ftemp) (FP32 inverse + one FP64 refinement
-// step r = dl - (x - gamma_lu J x), x += A r; FP64 inverse: no refinement),
-// scaled by 2 / (1 + gamrat) when gamma has moved since the setup; then
-// acor += x.  Returns the WRMS norms of x (*del) and of the new acor (*anrm).
+// dl = -(rl1 zn[1] + acor - gamma ftemp) (FP32 inverse, then, when `refine`,
+// one FP64 refinement step r = dl - (x - gamma_lu J x), x += A r, whose WRMS
+// relative to x goes to *ratio; FP64 inverse: no refinement), scaled by
+// 2 / (1 + gamrat) when gamma has moved since the setup; then acor += x.
+// Returns the WRMS norms of x (*del) and of the new acor (*anrm).
 // Internal status of a cell stopped for the FP64 retry (never reported).
 constexpr int kStatusRefineStall = -100;
+// refine_ratio of a cell whose current matrix has not been measured yet
+constexpr float kRefineUnknown = 3.0e38f;
 
 template <int n, int G, typename LUT>
 __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, const LUT* A, double rl1, double gamma,
                                          double gamma_lu, double gamrat, int gl, unsigned gm, double* del,
-                                         double* anrm, double stall_ratio, bool* stall) {
+                                         double* anrm, double stall_ratio, bool* stall, bool refine,
+                                         float* ratio) {
   constexpr int CPL = (n + G - 1) / G;
   double dl[CPL], x[CPL], dsc[CPL];
 #pragma unroll
@@ -501,39 +507,40 @@ __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, cons
   }
   g_apply_inverse<n, G, LUT>(A, dsc, x, gl, gm);
   if constexpr (sizeof(LUT) == 4) {
-    constexpr int LDJ = (n + 1) / 2 * 2;
-    double r[CPL];
+    if (refine) {
+      constexpr int LDJ = (n + 1) / 2 * 2;
+      double r[CPL];
 #pragma unroll
-    for (int cc = 0; cc < CPL; ++cc) r[cc] = 0.0;
+      for (int cc = 0; cc < CPL; ++cc) r[cc] = 0.0;
 #pragma unroll
-    for (int j = 0; j < n; ++j) {
-      const double xj = __shfl_sync(gm, x[j / G], j % G, G);
-      const double* col = J + j * LDJ;
+      for (int j = 0; j < n; ++j) {
+        const double xj = __shfl_sync(gm, x[j / G], j % G, G);
+        const double* col = J + j * LDJ;
+#pragma unroll
+        for (int cc = 0; cc < CPL; ++cc) {
+          const int i = gl + G * cc;
+          if (i < n) r[cc] += col[i] * xj;
+        }
+      }
+#pragma unroll
+      for (int cc = 0; cc < CPL; ++cc) r[cc] = dl[cc] - (x[cc] - gamma_lu * r[cc]);
+      g_apply_inverse<n, G, LUT>(A, dsc, r, gl, gm);
+      double r2 = 0.0, x2 = 0.0;
 #pragma unroll
       for (int cc = 0; cc < CPL; ++cc) {
         const int i = gl + G * cc;
-        if (i < n) r[cc] += col[i] * xj;
+        if (i < n) {
+          const double w = v.ewt(i);
+          r2 += (r[cc] * w) * (r[cc] * w);
+          x2 += (x[cc] * w) * (x[cc] * w);
+        }
+        x[cc] += r[cc];
       }
-    }
-#pragma unroll
-    for (int cc = 0; cc < CPL; ++cc) r[cc] = dl[cc] - (x[cc] - gamma_lu * r[cc]);
-    g_apply_inverse<n, G, LUT>(A, dsc, r, gl, gm);
-    double r2 = 0.0, x2 = 0.0;
-#pragma unroll
-    for (int cc = 0; cc < CPL; ++cc) {
-      const int i = gl + G * cc;
-      if (i < n) {
-        const double w = v.ewt(i);
-        r2 += (r[cc] * w) * (r[cc] * w);
-        x2 += (x[cc] * w) * (x[cc] * w);
-      }
-      x[cc] += r[cc];
-    }
-    // the refinement step must be small against the correction it refines
-    if (stall_ratio > 0.0) {
+      // the refinement step must be small against the correction it refines
       r2 = gsum<G>(r2, gm);
       x2 = gsum<G>(x2, gm);
-      *stall = !(r2 <= stall_ratio * stall_ratio * x2);
+      *ratio = (x2 > 0.0) ? (float)fmin(sqrt(r2 / x2), 1e30) : 0.0f;
+      if (stall_ratio > 0.0) *stall = !(r2 <= stall_ratio * stall_ratio * x2);
     }
   }
   const double sc = (gamrat != 1.0) ? 2.0 / (1.0 + gamrat) : 1.0;
@@ -561,7 +568,7 @@ __device__ __forceinline__ void g_newton(const RVec<n>& v, const double* J, cons
 template <int n, int G, typename LUT>
 __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, const double* atolv, double rtol,
                                          const double* J, const LUT* A, int gl, unsigned gm, int* status,
-                                         double stall_ratio = 0.0) {
+                                         double stall_ratio = 0.0, double keep_ratio = 0.0) {
   for (int guard = 0; guard < 256; ++guard) {
     switch (lab) {
       case kLAfterF0: {
@@ -709,6 +716,7 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
       }
       case kLAfterSetup: {
         c.callSetup = 0;
+        c.refine_ratio = kRefineUnknown;
         if (c.setup_ier) {
           lab = kLNlsFail2;
           break;
@@ -722,8 +730,14 @@ __device__ __forceinline__ int r_advance(RCell& c, const RVec<n>& v, int lab, co
         c.cnt.nni++;
         double del, anrm;
         bool stall = false;
+        // the FP64 refinement runs on the first correction with a new matrix,
+        // and again on every later one unless that first measurement showed
+        // the FP32 solve alone accurate to keep_ratio
+        const bool refine = !(keep_ratio > 0.0 && c.refine_ratio <= keep_ratio);
+        float ratio = c.refine_ratio;
         g_newton<n, G, LUT>(v, J, A, c.rl1, c.gamma, c.gamma_lu, c.gamrat, gl, gm, &del, &anrm, stall_ratio,
-                            &stall);
+                            &stall, refine, &ratio);
+        c.refine_ratio = ratio;
         if (stall) {
           // the FP32 inverse does not resolve this iteration matrix: the cell
           // is left untouched for the pass with the FP64 LU
@@ -873,6 +887,7 @@ __device__ __forceinline__ void r_begin(RCell& c, const RVec<n>& v, const double
   c.tn = 0.0;
   c.dt = dt;
   c.cnt = CellCounters{0, 0, 0, 0, 0, 0, 0};
+  c.refine_ratio = kRefineUnknown;
   c.nstlp = c.nstlj = 0;
   c.q = c.qprime = 1;
   c.L = 2;

@@ -70,9 +70,12 @@ struct ReactParams {
   // untouched and flags it in retry[cell] for a pass with the FP64 LU
   // (refine_stall <= 0: no check); retry_pass = 1 integrates only the
   // flagged cells
-  double refine_stall;
-  int* retry;
-  int retry_pass;
+  double refine_stall = 0.0;
+  // > 0: a Newton correction skips the FP64 refinement when the first
+  // correction with the same matrix measured the FP32 solve accurate to this
+  double refine_keep = 0.0;
+  int* retry = nullptr;
+  int retry_pass = 0;
 };
 
 __device__ __forceinline__ double* elem(const DevArr& a, int i, int j, int k) {

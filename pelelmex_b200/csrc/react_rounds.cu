@@ -461,15 +461,20 @@ __device__ __forceinline__ void ctrl_cell(const RoundsParams& R, bool live, int 
   if (live) {
     unsigned char* rec = rec_of(R.S, slot);
     if (B200_CTRL_PREFETCH >= 1 && gl == 0)
-      l2_prefetch(rec + R.S.L.off_vec, (uint32_t)(R.S.L.stride - R.S.L.off_vec));
+      l2_prefetch(rec + R.S.L.off_vec, (uint32_t)(R.S.L.off_j - R.S.L.off_vec));
     if (B200_CTRL_PREFETCH >= 2 && gl == 0 && idx_next >= 0)
       l2_prefetch(rec_of(R.S, R.list_in[idx_next]), (uint32_t)R.S.L.off_j);
     load_cell(c, rec);
+    // the Jacobian and the inverse only when this pass starts with a Newton
+    // iteration (a pass that ends in a setup would fetch them for nothing)
+    if (B200_CTRL_PREFETCH >= 1 && gl == 0 &&
+        (c.label == kLAfterNIter || c.label == kLAfterSetup || (c.label == kLAfterNStart && !c.callSetup)))
+      l2_prefetch(rec + R.S.L.off_j, (uint32_t)(R.S.L.stride - R.S.L.off_j));
     if (after_rhs) c.cnt.nfe++;
     const RVec<n> v{reinterpret_cast<double*>(rec + R.S.L.off_vec)};
     need = r_advance<n, G, LUT>(c, v, c.label, P.atol, P.rtol, reinterpret_cast<const double*>(rec + R.S.L.off_j),
                                 reinterpret_cast<const LUT*>(rec + R.S.L.off_a), gl, gm, &status,
-                                sizeof(LUT) == 4 ? P.refine_stall : 0.0);
+                                sizeof(LUT) == 4 ? P.refine_stall : 0.0, sizeof(LUT) == 4 ? P.refine_keep : 0.0);
     __syncwarp(gm);
     if (gl == 0) store_cell(c, rec);
     if (need == kDone) {

@@ -108,7 +108,7 @@ class ReactorB200:
 
     def __init__(self, mechanism=None, rtol: float = 1e-10, atol: float = 1e-10, max_order: int = 2,
                  max_steps: int = 10000, lu_fp64: bool = False, refine_stall_ppm: int = 0, kernel: str = "auto",
-                 setup_ratio: int = 0, ctas_per_sm: int = 0, group_lanes: int = 0):
+                 setup_ratio: int = 0, ctas_per_sm: int = 0, group_lanes: int = 0, refine_keep_ppm: int = 0):
         if mechanism is None:
             raise ValueError("a mechanism (name of a bundled file, path, or Mechanism) is required")
         if isinstance(mechanism, str) and not Path(mechanism).exists():
@@ -119,7 +119,7 @@ class ReactorB200:
         self.flat = mechmod.flatten(mechanism)
         self.N = self.flat.n_species
         self.opts = _lib.Opts(rtol, atol, max_order, max_steps, 2, 1 if lu_fp64 else 0, refine_stall_ppm, 0,
-                              self.KERNELS[kernel], setup_ratio, ctas_per_sm, group_lanes)
+                              self.KERNELS[kernel], setup_ratio, ctas_per_sm, group_lanes, refine_keep_ppm, 0)
         self._h = None
         self._typ = None
 
@@ -137,7 +137,8 @@ class ReactorB200:
                    refine_stall_ppm=int(params.get("b200.refine_stall_ppm", 0)),
                    kernel=params.get("b200.kernel", "auto"), setup_ratio=int(params.get("b200.setup_ratio", 0)),
                    ctas_per_sm=int(params.get("b200.ctas_per_sm", 0)),
-                   group_lanes=int(params.get("b200.group_lanes", 0)))
+                   group_lanes=int(params.get("b200.group_lanes", 0)),
+                   refine_keep_ppm=int(params.get("b200.refine_keep_ppm", 0)))
 
     def init(self, reactor_type: int = 2, ncells: int = 1):
         if reactor_type != 2:

@@ -26,14 +26,14 @@ def test_library_exports_all_declared_symbols():
     lib = ctypes.CDLL(str(build.build()))
     missing = [n for n in declared() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.b200chem_version() == 2
+    assert lib.b200chem_version() == 3
 
 
 def test_struct_layouts_match_header():
     from pelelmex_b200 import _lib
     assert ctypes.sizeof(_lib.Array4) == 8 + 3 * 8 + 6 * 4
     assert ctypes.sizeof(_lib.BoxView) == 24 + 7 * ctypes.sizeof(_lib.Array4)
-    assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 10 * 4  # two doubles and ten int32 fields
+    assert ctypes.sizeof(_lib.Opts) == 2 * 8 + 12 * 4  # two doubles and twelve int32 fields
     assert ctypes.sizeof(_lib.ChemBox) == 24 + 11 * ctypes.sizeof(_lib.Array4) + 8
     assert ctypes.sizeof(_lib.ForceBox) == 24 + 7 * ctypes.sizeof(_lib.Array4)
 

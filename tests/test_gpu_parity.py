@@ -38,10 +38,10 @@ def _dev(a, dtype=torch.float64):
 
 
 def run_gpu(name, f, rtol=1e-8, atol=1e-12, max_order=5, lu_fp64=False, typ=None, mask=None, max_steps=10000,
-            fY=None, fH=None, kernel="auto", group_lanes=0, refine_stall_ppm=0):
+            fY=None, fH=None, kernel="auto", group_lanes=0, refine_stall_ppm=0, refine_keep_ppm=0):
     r = ReactorB200(name, rtol=rtol, atol=atol, max_order=max_order, lu_fp64=lu_fp64,
                     max_steps=max_steps, kernel=kernel, group_lanes=group_lanes,
-                    refine_stall_ppm=refine_stall_ppm).init(2, f.ncells)
+                    refine_stall_ppm=refine_stall_ppm, refine_keep_ppm=refine_keep_ppm).init(2, f.ncells)
     if typ is not None:
         r.set_typ_vals_ode(typ)
     rhoY, T, rhoH = _dev(f.rhoY), _dev(f.T), _dev(f.rhoH)

@@ -144,3 +144,25 @@ def test_fp64_fallback_of_stalled_refinement(orc_cache):
     assert st["nfe"] == int(forced["fct"].sum())
     o = _oracle(orc_cache, name, f)
     compare(f, forced, o, "FP64 fallback forced")
+
+
+def test_adaptive_refinement_is_opt_in(orc_cache):
+    """refine_keep_ppm: by default every Newton correction is refined (the
+    result is bit-identical to refine_keep_ppm < 0); with a positive bound
+    the later corrections of a matrix whose FP32 solve measured accurate
+    skip the refinement.  The counters then stay within a fraction of a
+    percent of the oracle's, and the result within the integrator's own
+    error of the dense-direct solve (a few step decisions flip against the
+    FP64 solve, so the 1e-8 Y parity bar is not asserted for this mode)."""
+    mech = M.builtin("synth_ch4_21")
+    f = W.flame_ch4(mech, cells=W.sample_cells(128 ** 3, 4096, seed=31), dt=1e-5)
+    d = run_gpu("synth_ch4_21", f, kernel="rounds")
+    never = run_gpu("synth_ch4_21", f, kernel="rounds", refine_keep_ppm=-1)
+    assert np.array_equal(d["T"], never["T"]) and np.array_equal(d["rhoY"], never["rhoY"])
+    keep = run_gpu("synth_ch4_21", f, kernel="rounds", refine_keep_ppm=10)
+    o = _oracle(orc_cache, "synth_ch4_21", f)
+    assert (keep["status"] == 0).all()
+    assert np.max(np.abs(keep["T"] - o["T"]) / o["T"]) <= 1e-6
+    rho = f.rhoY.sum(axis=0)
+    assert (np.abs(keep["rhoY"] - o["rhoY"]).max(axis=0) / rho).max() <= 1e-7
+    assert abs(keep["stats"]["nfe"] - o["fct"].sum()) <= 0.005 * o["fct"].sum()
