@@ -1,6 +1,7 @@
 """Train, calibrate and save the surrogate ensemble of the hybrid reactor.
 
     python -m pelelmex_b200.train_surrogate --out pelelmex_b200/surrogates/synth_ch4_21.b2s
+    python -m pelelmex_b200.train_surrogate --recalibrate FILE --out FILE   # new rule, same networks
 
 1. Training fields: the drm19-shaped 128^3 flame field (workloads.flame_ch4)
    for seeds 10..15, generated on the host cores (a process pool started
@@ -9,13 +10,15 @@
    (state, dt) -> state pairs.
 2. Training: `members` networks on the tensor cores (surrogate.train_ensemble),
    each on its own random 80 % of the pairs.
-3. Calibration of the acceptance rule on a held-out field (seed 5, never
-   trained on): for each candidate rule, b200chem_react_hybrid reacts the
-   field at both time steps and the largest temperature error of an accepted
-   cell against the plain BDF is measured; the most permissive rule whose
-   worst accepted cell stays within `margin` of the 1e-4 bar at both time
-   steps is kept (the candidates are ordered from strict to permissive; if
-   none does, the strictest is stored and the report says so).
+3. Calibration of the acceptance rule on held-out fields (seeds 5 and 6,
+   never trained on): every candidate rule of a (spread, dT_cap, gap) grid
+   reacts each field at both time steps through b200chem_react_hybrid, and
+   the largest temperature error of an accepted cell against the plain BDF is
+   measured.  Kept: among the rules whose worst accepted cell stays within
+   `margin` of the 1e-4 bar on every field and time step, the one that takes
+   the most right-hand-side work off the BDF (if none does, the strictest is
+   stored and the report says so).  The bench field (seed 2) is not among
+   them, so the bench's error is an independent test of the rule.
 4. The versioned weights file (the format of b200chem_surrogate_load) carries
    the networks, their normalisation, the element matrix and the rule.
 """
@@ -32,9 +35,9 @@ import numpy as np
 
 EDGE = 128
 
-# candidate acceptance rules, strict to permissive: (spread, dT_cap, gap) in bars
-CANDIDATES = [(0.02, 3.0, 1.5), (0.03, 5.0, 2.0), (0.05, 5.0, 3.0), (0.05, 10.0, 3.0), (0.08, 10.0, 3.0), (0.1, 10.0, 3.0),
-              (0.1, 15.0, 3.0), (0.12, 15.0, 3.0), (0.15, 15.0, 3.0), (0.15, 20.0, 3.0), (0.2, 20.0, 5.0)]
+# candidate acceptance rules: (spread, dT_cap, gap) in bars, the strictest first
+CANDIDATES = [(sp, cap, gap) for sp in (0.03, 0.05, 0.08, 0.1, 0.15, 0.2, 0.25) for cap in (10.0, 15.0, 20.0)
+              for gap in (1.0, 1.5, 3.0)]
 
 
 def _gen(a):
@@ -57,9 +60,11 @@ def flame_fields(pool, name, seeds, edge=EDGE, chunks=64):
 
 
 def calibrate(reactor, ens, fields, dts, margin, log=print):
-    """Pick the most permissive candidate rule whose worst accepted cell stays
-    within `margin` bars at every dt on the held-out fields.  Returns the rule
-    and the per-candidate table."""
+    """Among the candidate rules whose worst accepted cell stays within
+    `margin` bars at every dt on every held-out field, pick the one that saves
+    the most BDF work (right-hand sides of the accepted cells, summed over
+    fields and time steps).  Returns the rule (None if no candidate
+    qualifies), the per-candidate table and the worst cells of each."""
     import torch
     from .surrogate import HybridOpts, HybridReactor
     dev = torch.device("cuda:0")
@@ -71,25 +76,25 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
             fct = torch.zeros_like(a[1])
             reactor.react_flat(a[0], fY, a[1], a[2], fH, fct, dt_react=dt)
             plain[(key, dt)] = (a[1], fct)
-    table, best, worst = [], None, {}
+    table, best, best_saved, worst = [], None, -1.0, {}
     for spread, cap, gap in CANDIDATES:
         opts = HybridOpts(spread=spread, dT_cap=cap, gap=gap)
         row = {"spread": spread, "dT_cap": cap, "gap": gap}
         ok_all = True
+        saved_all = 0.0
         for key, (rY, T, rH) in fields.items():
             for dt in dts:
                 a = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
                 fY, fH = torch.zeros_like(a[0]), torch.zeros_like(a[1])
-                h = HybridReactor(reactor, ens, opts)
-                h.react_flat(a[0], fY, a[1], a[2], fH, None, dt_react=dt)
                 T_ref, fct = plain[(key, dt)]
+                hf = torch.zeros_like(fct)
+                h = HybridReactor(reactor, ens, opts)
+                h.react_flat(a[0], fY, a[1], a[2], fH, hf, dt_react=dt)
                 e = (a[1] - T_ref) / (opts.t_rel * T_ref)
                 err = e.abs().max().item()
                 acc = h.last["accepted"] / h.last["predicted"]
-                # cost the BDF no longer spends: right-hand sides of the accepted cells
-                hf = torch.zeros_like(fct)
-                a2 = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
-                h.react_flat(a2[0], fY, a2[1], a2[2], fH, hf, dt_react=dt)
+                # cost the BDF no longer spends: right-hand sides of the accepted
+                # cells (an accepted cell's count is 0)
                 saved = (fct[hf == 0].sum() / fct.sum()).item()
                 h.close()
                 row[f"{key}_dt{dt:g}"] = {"accepted": round(acc, 4), "bdf_cost_saved": round(saved, 4),
@@ -100,11 +105,12 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
                     (int(c), int(c) % EDGE, round(float(T[int(c)]), 1), round(float(e[int(c)]), 3))
                     for c in top.indices.tolist()]
                 ok_all &= err <= margin
+                saved_all += saved
         row["within_margin"] = bool(ok_all)
         table.append(row)
         log(json.dumps(row))
-        if ok_all:
-            best = opts
+        if ok_all and saved_all > best_saved:
+            best, best_saved = opts, saved_all
     return best, table, worst
 
 
@@ -113,17 +119,20 @@ def main():
     p.add_argument("--mechanism", default="synth_ch4_21")
     p.add_argument("--out", required=True)
     p.add_argument("--seeds", default="10,11,12,13,14,15", help="training field seeds")
-    p.add_argument("--val-seed", type=int, default=5, help="held-out calibration field seed")
+    p.add_argument("--val-seeds", default="5,6", help="held-out calibration field seeds")
+    p.add_argument("--recalibrate", default=None,
+                   help="weights file whose networks are kept: only the acceptance rule is calibrated again")
     p.add_argument("--members", type=int, default=8)
     p.add_argument("--steps", type=int, default=20000)
     p.add_argument("--batch", type=int, default=16384)
-    p.add_argument("--margin", type=float, default=0.75, help="worst accepted cell allowed, in bars")
+    p.add_argument("--margin", type=float, default=0.8, help="worst accepted cell allowed, in bars")
     p.add_argument("--report", default=None, help="JSON file for the calibration table")
     a = p.parse_args()
-    seeds = [int(s) for s in a.seeds.split(",")]
+    seeds = [] if a.recalibrate else [int(s) for s in a.seeds.split(",")]
+    val = [int(s) for s in a.val_seeds.split(",")]
     t0 = time.time()
     with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
-        fields = flame_fields(pool, a.mechanism, seeds + [a.val_seed])
+        fields = flame_fields(pool, a.mechanism, seeds + val)
     print(f"fields generated in {time.time() - t0:.1f} s", flush=True)
 
     import torch
@@ -133,15 +142,19 @@ def main():
     mech = M.builtin(a.mechanism)
     r = ReactorB200(mech, rtol=1e-8, atol=1e-12, max_order=5).init()
     dts = (1e-6, 1e-5)
-    t1 = time.time()
-    train = [SimpleNamespace(rhoY=fields[s][0], T=fields[s][1], rhoH=fields[s][2], dt=dt) for s in seeds
-             for dt in dts]
-    nets = train_ensemble(r, mech, train, members=a.members, steps=a.steps, batch=a.batch,
-                          log=lambda m: print(m, f"({time.time() - t1:.0f} s)", flush=True))
-    torch.cuda.synchronize()
-    print(f"trained {a.members} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
-    ens = Ensemble(nets)
-    rule, table, worst = calibrate(r, ens, {f"seed{a.val_seed}": fields[a.val_seed]}, dts, a.margin)
+    if a.recalibrate:
+        ens = Ensemble.load(a.recalibrate, mech)
+        print(f"loaded {len(ens.members)} networks from {a.recalibrate}", flush=True)
+    else:
+        t1 = time.time()
+        train = [SimpleNamespace(rhoY=fields[s][0], T=fields[s][1], rhoH=fields[s][2], dt=dt) for s in seeds
+                 for dt in dts]
+        nets = train_ensemble(r, mech, train, members=a.members, steps=a.steps, batch=a.batch,
+                              log=lambda m: print(m, f"({time.time() - t1:.0f} s)", flush=True))
+        torch.cuda.synchronize()
+        print(f"trained {a.members} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
+        ens = Ensemble(nets)
+    rule, table, worst = calibrate(r, ens, {f"seed{v}": fields[v] for v in val}, dts, a.margin)
     within = rule is not None
     if not within:
         from .surrogate import HybridOpts
@@ -160,8 +173,8 @@ def main():
     if a.report:
         with open(a.report, "w") as f:
             json.dump({"rule": rule.__dict__, "within_margin": within, "margin_bars": a.margin, "table": table,
-                       "members": a.members, "steps": a.steps, "train_seeds": seeds, "val_seed": a.val_seed,
-                       "dts": dts}, f, indent=1)
+                       "members": len(ens.members), "steps": None if a.recalibrate else a.steps,
+                       "train_seeds": seeds or None, "val_seeds": val, "dts": dts}, f, indent=1)
     r.close()
 
 
