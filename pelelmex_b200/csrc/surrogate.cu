@@ -483,9 +483,55 @@ __device__ __forceinline__ double grp_max(double v, unsigned gm) {
   return v;
 }
 
-template <int NS, int G>
-__global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
+// Solves G x = b in place (b -> x) for a symmetric positive semi-definite G
+// given by its lower triangle, by an LDL^T factorisation without pivoting,
+// fully unrolled so that G stays in registers (G is overwritten with L).  A
+// column whose pivot falls to 1e-13 of its diagonal or below (a constraint
+// row that vanishes, or that the others already fix) is dropped: its
+// unknown is 0, as the pivoted Gauss-Jordan of hy_gate skips a zero pivot.
+template <int NR>
+__device__ __forceinline__ void ldl_solve(double (&Gm)[NR][NR], double (&b)[NR]) {
+  double D[NR];
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+    double dj = Gm[j][j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) dj -= Gm[j][k] * Gm[j][k] * D[k];
+    const bool keep = dj > 1e-13 * Gm[j][j] && dj > 0.0;
+    D[j] = keep ? dj : 0.0;
+    const double inv = keep ? 1.0 / dj : 0.0;
+#pragma unroll
+    for (int i = j + 1; i < NR; ++i) {
+      double v = Gm[i][j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v -= Gm[i][k] * Gm[j][k] * D[k];
+      Gm[i][j] = v * inv;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NR; ++j) {
+#pragma unroll
+    for (int k = 0; k < j; ++k) b[j] -= Gm[j][k] * b[k];
+  }
+#pragma unroll
+  for (int j = 0; j < NR; ++j) b[j] = D[j] > 0.0 ? b[j] / D[j] : 0.0;
+#pragma unroll
+  for (int j = NR - 1; j >= 0; --j) {
+#pragma unroll
+    for (int i = j + 1; i < NR; ++i) b[j] -= Gm[i][j] * b[i];
+  }
+}
+
+// Minimum resident CTAs per SM requested for the lane-group gate (bounds its
+// registers per thread).
+#ifndef B200_GATE_MIN_CTAS
+#define B200_GATE_MIN_CTAS 3
+#endif
+
+template <int NS, int G, int NR>
+__global__ void __launch_bounds__(128, B200_GATE_MIN_CTAS) hy_gate_grp(GateParams P) {
   constexpr int n = NS + 1;
+  constexpr int NE = NR - 1;  // elements
   constexpr int CPL = (n + G - 1) / G;
   constexpr int kout = sg_out(NS);
   __shared__ DevMech s_mech;
@@ -504,12 +550,12 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
     int reason = kAccept;
     if (in && !masked) {
       // this lane's components: j = gl + G cc (0: T, k + 1: species k)
-      double y0[CPL], F[CPL], d[CPL], z[CPL], hk[CPL], a_row[CPL];
+      double y0[CPL], F[CPL], d[CPL], z[CPL];
       double rs = 0.0;
 #pragma unroll
       for (int cc = 0; cc < CPL; ++cc) {
         const int j = gl + G * cc;
-        y0[cc] = F[cc] = d[cc] = z[cc] = hk[cc] = 0.0;
+        y0[cc] = F[cc] = d[cc] = z[cc] = 0.0;
         if (j >= 1 && j < n) {
           y0[cc] = P.rhoY[(long long)(j - 1) * P.ld + c];
           F[cc] = P.fY[(long long)(j - 1) * P.ld + c];
@@ -571,22 +617,28 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
       bad = grp_max<G>(bad ? 1.0 : 0.0, gm) > 0.0;
       if (!reason && bad) reason = kRejNonfinite;
       if (!reason && !(fabs(zs - rho1t) <= P.o.tol_mass * rho1t)) reason = kRejMass;
-      const int ne = P.ne < kMaxElem ? P.ne : kMaxElem;
-      double tgt[kMaxElem + 1], rsc[kMaxElem + 1];
+      // constraint rows on this lane's components: A[e] the element e
+      // content (mol per gram of species), A[NE] the species enthalpy at T1;
+      // each row scaled by rsc (unit max-norm) in the projection
+      double A[NR][CPL], tgt[NR], rsc[NR];
       const double rhoH1 = P.rhoH[c] + P.dt * FH;
+      double tot = 0.0;
       if (!reason) {
-        double tot = 0.0, worst = 0.0;
-        for (int e = 0; e < ne; ++e) {
+        double worst = 0.0;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
           double ct = 0.0, cz = 0.0, mx = 0.0;
 #pragma unroll
           for (int cc = 0; cc < CPL; ++cc) {
             const int j = gl + G * cc;
+            double a = 0.0;
             if (j >= 1 && j < n) {
-              const double a = __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1));
+              a = __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1));
               ct += a * (y0[cc] + P.dt * F[cc]);
               cz += a * z[cc];
               mx = fmax(mx, fabs(a));
             }
+            A[e][cc] = a;
           }
           ct = grp_sum<G>(ct, gm);
           cz = grp_sum<G>(cz, gm);
@@ -639,86 +691,55 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
 #pragma unroll
         for (int cc = 0; cc < CPL; ++cc) {
           const int j = gl + G * cc;
+          double a = 0.0;
           if (j >= 1 && j < n) {
             double cpR, hRT, sR, dcpR;
             nasa7(m, j - 1, T1, lnT1, cpR, hRT, sR, dcpR);
-            hk[cc] = hRT * kRu * T1 * __ldg(m.inv_mw + (j - 1));
-            mx = fmax(mx, fabs(hk[cc]));
+            a = hRT * kRu * T1 * __ldg(m.inv_mw + (j - 1));
+            mx = fmax(mx, fabs(a));
           }
+          A[NE][cc] = a;
         }
         mx = grp_max<G>(mx, gm);
-        tgt[ne] = rhoH1;
-        rsc[ne] = mx > 0.0 ? 1.0 / mx : 0.0;
+        tgt[NE] = rhoH1;
+        rsc[NE] = mx > 0.0 ? 1.0 / mx : 0.0;
         // weighted minimum-norm correction z' = z - W A^T (A W A^T)^-1 (A z - b)
-        // over the ne + 1 scaled rows A, the passes of hy_gate
-        const int nr = ne + 1;
+        // over the NR scaled rows, the passes of hy_gate, with the small
+        // symmetric system solved by an LDL^T factorisation in registers
         unsigned frozen = 0;  // bit cc: this lane's component cc is frozen at zero
         bool clipped = true;
         for (int pass = 0; pass < kMaxPasses && !reason && (pass < kMinPasses || clipped); ++pass) {
-          double Gm[kMaxElem + 1][kMaxElem + 1], lam[kMaxElem + 1];
-          for (int e = 0; e < nr; ++e) {
+          double w[CPL];
 #pragma unroll
-            for (int cc = 0; cc < CPL; ++cc) {
-              const int j = gl + G * cc;
-              a_row[cc] = 0.0;
-              if (j >= 1 && j < n)
-                a_row[cc] = (e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) *
-                            rsc[e];
-            }
+          for (int cc = 0; cc < CPL; ++cc) {
+            const int j = gl + G * cc;
+            w[cc] = (j >= 1 && j < n && !((frozen >> cc) & 1u)) ? fmax(fabs(z[cc]), 1e-10 * rho0) : 0.0;
+          }
+          double Gm[NR][NR], lam[NR];
+#pragma unroll
+          for (int e = 0; e < NR; ++e) {
             double az = 0.0;
 #pragma unroll
-            for (int cc = 0; cc < CPL; ++cc) az += a_row[cc] * z[cc];
-            lam[e] = grp_sum<G>(az, gm) - tgt[e] * rsc[e];
+            for (int cc = 0; cc < CPL; ++cc) az += A[e][cc] * z[cc];
+            lam[e] = (grp_sum<G>(az, gm) - tgt[e]) * rsc[e];
+#pragma unroll
             for (int f = 0; f <= e; ++f) {
               double g = 0.0;
 #pragma unroll
-              for (int cc = 0; cc < CPL; ++cc) {
-                const int j = gl + G * cc;
-                if (j >= 1 && j < n && !((frozen >> cc) & 1u)) {
-                  const double af = (f < ne ? __ldg(P.elem + f * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) *
-                                    rsc[f];
-                  g += a_row[cc] * af * fmax(fabs(z[cc]), 1e-10 * rho0);
-                }
-              }
-              Gm[e][f] = Gm[f][e] = grp_sum<G>(g, gm);
+              for (int cc = 0; cc < CPL; ++cc) g += A[e][cc] * A[f][cc] * w[cc];
+              Gm[e][f] = grp_sum<G>(g, gm) * rsc[e] * rsc[f];
             }
           }
-          // Gauss-Jordan with partial pivoting (singular pivots: row skipped)
-          for (int col = 0; col < nr; ++col) {
-            int piv = col;
-            for (int w = col + 1; w < nr; ++w)
-              if (fabs(Gm[w][col]) > fabs(Gm[piv][col])) piv = w;
-            if (!(fabs(Gm[piv][col]) > 1e-300)) continue;
-            if (piv != col) {
-              for (int w = 0; w < nr; ++w) {
-                const double t = Gm[col][w];
-                Gm[col][w] = Gm[piv][w];
-                Gm[piv][w] = t;
-              }
-              const double t = lam[col];
-              lam[col] = lam[piv];
-              lam[piv] = t;
-            }
-            const double inv = 1.0 / Gm[col][col];
-            for (int w = 0; w < nr; ++w) {
-              if (w == col) continue;
-              const double f = Gm[w][col] * inv;
-              if (f == 0.0) continue;
-              for (int v = col; v < nr; ++v) Gm[w][v] -= f * Gm[col][v];
-              lam[w] -= f * lam[col];
-            }
-          }
-          for (int e = 0; e < nr; ++e) lam[e] = (fabs(Gm[e][e]) > 1e-300) ? lam[e] / Gm[e][e] : 0.0;
+          ldl_solve<NR>(Gm, lam);
           bool neg = false, clip = false;
 #pragma unroll
           for (int cc = 0; cc < CPL; ++cc) {
             const int j = gl + G * cc;
             if (j >= 1 && j < n && !((frozen >> cc) & 1u)) {
               double corr = 0.0;
-              for (int e = 0; e < nr; ++e)
-                corr += (e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc]) * rsc[e] *
-                        lam[e];
-              z[cc] -= fmax(fabs(z[cc]), 1e-10 * rho0) * corr;
+#pragma unroll
+              for (int e = 0; e < NR; ++e) corr += A[e][cc] * rsc[e] * lam[e];
+              z[cc] -= w[cc] * corr;
               if (z[cc] < -P.o.tol_mass * rho1t) neg = true;
               if (z[cc] < 0.0) {
                 z[cc] = 0.0;
@@ -733,22 +754,17 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
         if (!reason && clipped) reason = kRejNegative;
         // every constraint met to round-off, or the cell goes to the BDF
         // (the scales of hy_gate)
-        double tot = 0.0;
-        for (int e = 0; e < ne; ++e) tot += tgt[e];
-        for (int e = 0; e < nr && !reason; ++e) {
+#pragma unroll
+        for (int e = 0; e < NR; ++e) {
           double az = 0.0, sc = 0.0;
 #pragma unroll
           for (int cc = 0; cc < CPL; ++cc) {
-            const int j = gl + G * cc;
-            if (j >= 1 && j < n) {
-              const double a = e < ne ? __ldg(P.elem + e * NS + (j - 1)) * __ldg(m.inv_mw + (j - 1)) : hk[cc];
-              az += a * z[cc];
-              sc += fabs(a) * z[cc];
-            }
+            az += A[e][cc] * z[cc];
+            sc += fabs(A[e][cc]) * z[cc];
           }
           az = grp_sum<G>(az, gm);
           sc = grp_sum<G>(sc, gm);
-          if (!(fabs(az - tgt[e]) <= kConsTol * (e < ne ? tot : sc))) reason = kRejElem;
+          if (!reason && !(fabs(az - tgt[e]) <= kConsTol * (e < NE ? tot : sc))) reason = kRejElem;
         }
       }
       if (!reason) {
@@ -786,14 +802,30 @@ __global__ void __launch_bounds__(128) hy_gate_grp(GateParams P) {
   }
 }
 
-template <int NS>
-int launch_gate_grp(const GateParams& P, int sm_count, cudaStream_t st) {
+template <int NS, int NR>
+int launch_gate_grp_nr(const GateParams& P, int sm_count, cudaStream_t st) {
   constexpr int G = NS + 1 <= 32 ? 8 : 16;
   const int per_block = 128 / G;
   const long long need = (P.nc + per_block - 1) / per_block;
   const long long cap = 32LL * sm_count;
-  hy_gate_grp<NS, G><<<(unsigned)(need < cap ? need : cap), 128, 0, st>>>(P);
+  hy_gate_grp<NS, G, NR><<<(unsigned)(need < cap ? need : cap), 128, 0, st>>>(P);
   return cudaGetLastError() == cudaSuccess ? 0 : B200CHEM_ECUDA;
+}
+
+// One instantiation per constraint count (elements + the energy).
+template <int NS>
+int launch_gate_grp(const GateParams& P, int sm_count, cudaStream_t st) {
+  switch ((P.ne < kMaxElem ? P.ne : kMaxElem) + 1) {
+    case 1: return launch_gate_grp_nr<NS, 1>(P, sm_count, st);
+    case 2: return launch_gate_grp_nr<NS, 2>(P, sm_count, st);
+    case 3: return launch_gate_grp_nr<NS, 3>(P, sm_count, st);
+    case 4: return launch_gate_grp_nr<NS, 4>(P, sm_count, st);
+    case 5: return launch_gate_grp_nr<NS, 5>(P, sm_count, st);
+    case 6: return launch_gate_grp_nr<NS, 6>(P, sm_count, st);
+    case 7: return launch_gate_grp_nr<NS, 7>(P, sm_count, st);
+    case 8: return launch_gate_grp_nr<NS, 8>(P, sm_count, st);
+    default: return launch_gate_grp_nr<NS, 9>(P, sm_count, st);
+  }
 }
 
 // The lane-group gate unless the residual check (a per-cell right-hand
