@@ -59,6 +59,22 @@ def flame_fields(pool, name, seeds, edge=EDGE, chunks=64):
     return out
 
 
+def pick_rule(table, margin):
+    """The calibration's choice: among the rows of `table` (one per candidate,
+    with a {"accepted", "bdf_cost_saved", "max_err_bars"} entry per field and
+    time step) whose worst accepted cell is within `margin` bars everywhere,
+    the one with the largest BDF work saved, summed over its entries (the
+    first such row on a tie).  Returns (spread, dT_cap, gap), or None."""
+    best, best_saved = None, -1.0
+    for row in table:
+        runs = [v for v in row.values() if isinstance(v, dict)]
+        if runs and all(v["max_err_bars"] <= margin for v in runs):
+            saved = sum(v["bdf_cost_saved"] for v in runs)
+            if saved > best_saved:
+                best, best_saved = (row["spread"], row["dT_cap"], row["gap"]), saved
+    return best
+
+
 def calibrate(reactor, ens, fields, dts, margin, log=print):
     """Among the candidate rules whose worst accepted cell stays within
     `margin` bars at every dt on every held-out field, pick the one that saves
@@ -76,12 +92,11 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
             fct = torch.zeros_like(a[1])
             reactor.react_flat(a[0], fY, a[1], a[2], fH, fct, dt_react=dt)
             plain[(key, dt)] = (a[1], fct)
-    table, best, best_saved, worst = [], None, -1.0, {}
+    table, worst = [], {}
     for spread, cap, gap in CANDIDATES:
         opts = HybridOpts(spread=spread, dT_cap=cap, gap=gap)
         row = {"spread": spread, "dT_cap": cap, "gap": gap}
         ok_all = True
-        saved_all = 0.0
         for key, (rY, T, rH) in fields.items():
             for dt in dts:
                 a = [torch.tensor(x, device=dev) for x in (rY, T, rH)]
@@ -105,12 +120,11 @@ def calibrate(reactor, ens, fields, dts, margin, log=print):
                     (int(c), int(c) % EDGE, round(float(T[int(c)]), 1), round(float(e[int(c)]), 3))
                     for c in top.indices.tolist()]
                 ok_all &= err <= margin
-                saved_all += saved
         row["within_margin"] = bool(ok_all)
         table.append(row)
         log(json.dumps(row))
-        if ok_all and saved_all > best_saved:
-            best, best_saved = opts, saved_all
+    key = pick_rule(table, margin)
+    best = None if key is None else HybridOpts(spread=key[0], dT_cap=key[1], gap=key[2])
     return best, table, worst
 
 

@@ -132,6 +132,27 @@ def test_weights_file_header_and_round_trip():
         Ensemble.from_bytes(data, M.builtin("synth_h2_9"), device="cpu")
 
 
+def test_calibration_picks_the_rule_that_saves_most_within_the_margin():
+    """The calibration's choice on a hand-made table: rules with any run over
+    the margin are out, the rest ranked by BDF work saved over every field and
+    time step, ties to the earlier (stricter) rule."""
+    from pelelmex_b200.train_surrogate import CANDIDATES, pick_rule
+
+    def row(rule, *runs):
+        r = {"spread": rule[0], "dT_cap": rule[1], "gap": rule[2]}
+        for i, (saved, err) in enumerate(runs):
+            r[f"seed{i}_dt1e-06"] = {"accepted": saved, "bdf_cost_saved": saved, "max_err_bars": err}
+        return r
+    table = [row((0.03, 10, 1), (0.30, 0.2), (0.20, 0.3)),
+             row((0.05, 10, 3), (0.45, 0.4), (0.20, 0.79)),
+             row((0.08, 20, 1.5), (0.55, 0.5), (0.30, 0.81)),   # one run over the margin
+             row((0.1, 10, 1), (0.40, 0.1), (0.25, 0.1))]       # saves 0.65, same as the second
+    assert pick_rule(table, 0.8) == (0.05, 10, 3)
+    assert pick_rule(table, 0.85) == (0.08, 20, 1.5)
+    assert pick_rule(table, 0.05) is None
+    assert (0.08, 20.0, 1.5) in CANDIDATES and CANDIDATES[0] == min(CANDIDATES)
+
+
 def _cells(n, seed, dt):
     from pelelmex_b200 import mechanism as M, workloads as W
     mech = M.builtin("synth_ch4_21")
