@@ -481,6 +481,38 @@ def train_ensemble(reactor, mech, fields, members=4, steps=8000, batch=16384, lr
     return nets
 
 
+def finetune_ensemble(reactor, ens, fields, steps=8000, batch=16384, lr=2e-4, lr_end=2e-6, seed=100, t_weight=None,
+                      bag=0.8, log=None):
+    """Continue training every member of `ens` on BDF-labelled `fields`, in
+    the ensemble's own normalisation (inputs and targets are encoded with the
+    statistics stored in its weights file, so the file format and the gate's
+    decoding are unchanged), with a fresh Adam state and a cosine learning
+    rate from `lr` to `lr_end`; each member on its own random share `bag` of
+    the pairs."""
+    torch = _torch()
+    s0 = ens.s
+    xs, ys = [], []
+    for f in fields:
+        rY, T, dy, _ = label_pairs(reactor, f)
+        nc = T.shape[0]
+        xs.append(s0.features(reactor, rY, T, f.dt, (nc + 127) // 128 * 128)[:nc])
+        ys.append(s0.encode(dy))
+    x, y = torch.cat(xs), torch.cat(ys)
+    del xs, ys
+    w = torch.ones(s0.nout, device=s0.device)
+    w[0] = float(t_weight if t_weight is not None else s0.N)
+    S = x.shape[0]
+    for mbr, s in enumerate(ens.members):
+        s._adam = None
+        gen = torch.Generator(device=s.device).manual_seed(2000 + seed + mbr)
+        sub = torch.randperm(S, device=s.device, generator=gen)[: int(bag * S)]
+        hist = s.train(x[sub], y[sub], steps=steps, batch=batch, lr=lr, lr_end=lr_end, weights=w,
+                       seed=seed + 7 * mbr, log_every=max(1, steps // 4))
+        if log:
+            log(f"member {mbr}: loss {[round(h[1], 5) for h in hist]}")
+    return ens
+
+
 class HybridReactor:
     """Surrogate-first reaction advance with gated fallback to the BDF: one
     library call (b200chem_react_hybrid) per react."""

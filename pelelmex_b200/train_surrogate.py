@@ -2,6 +2,7 @@
 
     python -m pelelmex_b200.train_surrogate --out pelelmex_b200/surrogates/synth_ch4_21.b2s
     python -m pelelmex_b200.train_surrogate --recalibrate FILE --out FILE   # new rule, same networks
+    python -m pelelmex_b200.train_surrogate --init FILE --steps 8000 --out FILE   # continue training
 
 1. Training fields: the drm19-shaped 128^3 flame field (workloads.flame_ch4)
    for seeds 10..15, generated on the host cores (a process pool started
@@ -136,6 +137,11 @@ def main():
     p.add_argument("--val-seeds", default="5,6", help="held-out calibration field seeds")
     p.add_argument("--recalibrate", default=None,
                    help="weights file whose networks are kept: only the acceptance rule is calibrated again")
+    p.add_argument("--init", default=None,
+                   help="weights file whose networks continue training (their normalisation is kept), then "
+                        "the rule is calibrated")
+    p.add_argument("--lr", type=float, default=None,
+                   help="initial learning rate (default 2e-3 from scratch, 2e-4 with --init)")
     p.add_argument("--members", type=int, default=8)
     p.add_argument("--steps", type=int, default=20000)
     p.add_argument("--batch", type=int, default=16384)
@@ -159,11 +165,21 @@ def main():
     if a.recalibrate:
         ens = Ensemble.load(a.recalibrate, mech)
         print(f"loaded {len(ens.members)} networks from {a.recalibrate}", flush=True)
+    elif a.init:
+        from .surrogate import finetune_ensemble
+        ens = Ensemble.load(a.init, mech)
+        t1 = time.time()
+        train = [SimpleNamespace(rhoY=fields[s][0], T=fields[s][1], rhoH=fields[s][2], dt=dt) for s in seeds
+                 for dt in dts]
+        finetune_ensemble(r, ens, train, steps=a.steps, batch=a.batch, lr=a.lr or 2e-4,
+                          log=lambda m: print(m, f"({time.time() - t1:.0f} s)", flush=True))
+        torch.cuda.synchronize()
+        print(f"continued {len(ens.members)} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
     else:
         t1 = time.time()
         train = [SimpleNamespace(rhoY=fields[s][0], T=fields[s][1], rhoH=fields[s][2], dt=dt) for s in seeds
                  for dt in dts]
-        nets = train_ensemble(r, mech, train, members=a.members, steps=a.steps, batch=a.batch,
+        nets = train_ensemble(r, mech, train, members=a.members, steps=a.steps, batch=a.batch, lr=a.lr or 2e-3,
                               log=lambda m: print(m, f"({time.time() - t1:.0f} s)", flush=True))
         torch.cuda.synchronize()
         print(f"trained {a.members} x {a.steps} steps in {time.time() - t1:.1f} s", flush=True)
@@ -188,6 +204,7 @@ def main():
         with open(a.report, "w") as f:
             json.dump({"rule": rule.__dict__, "within_margin": within, "margin_bars": a.margin, "table": table,
                        "members": len(ens.members), "steps": None if a.recalibrate else a.steps,
+                       "init": a.init,
                        "train_seeds": seeds or None, "val_seeds": val, "dts": dts}, f, indent=1)
     r.close()
 
